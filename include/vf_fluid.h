@@ -1,0 +1,153 @@
+/* vf_fluid.h — C ABI of the B200 CA-water engine (drop-in for the reference's FluidSim).
+ *
+ * The reference's fluid (src/fluid.rs:230-721) is a Rust struct `FluidSim` whose methods borrow
+ * the world (`&mut SparseVolume`). This ABI keeps those methods one to one; the world lives on
+ * the device as a brick table + atlases mirrored from the host's SparseVolume at
+ * vf_fluid_upload_world, and every voxel the fluid changes is handed back to the host by
+ * vf_fluid_download_changes so the host replays it through SparseVolume::set_voxel (which
+ * feeds the renderer's dirty_grid, src/voxel/sparse_volume.rs:289-291).
+ *
+ * Conventions follow the reference's own FFI layer (native/ngx_shim.cpp:18-45,
+ * src/gfx/dlss/ngx.rs:23-38): `vf_`-prefixed extern "C" functions returning int (0 = OK,
+ * negative = error), opaque handles, out-parameters, explicit destroy. A handle is not
+ * thread-safe, like the reference's `&mut self`; one handle per CUDA stream.
+ *
+ * Results are bit-identical to fluid.rs semantics: f32 volumes, f64 level sums, the same FIFO
+ * order, 50k-cell cap, pull budget, levelling rounds and seed order.
+ */
+#ifndef VF_FLUID_H
+#define VF_FLUID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes */
+#define VF_OK 0
+#define VF_ERR_INVALID (-1)   /* bad argument / handle */
+#define VF_ERR_OOM (-2)       /* device or host allocation failed, or a fixed capacity is full */
+#define VF_ERR_CUDA (-3)      /* a CUDA call failed (vf_fluid_last_error has the text) */
+#define VF_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up (the sim state is undefined) */
+#define VF_ERR_RANGE (-5)     /* a coordinate outside the addressable domain */
+#define VF_ERR_NO_DEVICE (-6) /* no CUDA device / the sm_100a image cannot load */
+#define VF_ERR_STATE (-7)     /* call not valid in the current state (e.g. tick before upload) */
+
+/* ---- constants of the reference (src/fluid.rs:24-44) */
+#define VF_FLUID_WATER 5
+#define VF_FLUID_TICK_HZ 20.0f
+#define VF_FLUID_MAX_CELLS_PER_TICK 50000
+#define VF_FLUID_MAX_PULLS_PER_TICK 4096
+#define VF_FLUID_LEVEL_BUDGET 40000
+#define VF_FLUID_MAX_LEVEL_SEEDS 4096
+#define VF_FLUID_MAX_LEVEL_CELLS 400000
+
+typedef struct vf_fluid vf_fluid;
+
+typedef struct vf_fluid_desc {
+  int32_t device;          /* CUDA device ordinal */
+  void* stream;            /* cudaStream_t to run on (NULL = the handle creates its own) */
+  uint64_t atlas_bricks;   /* capacity of the device brick atlas (0 = sized from the world) */
+  uint64_t queue_capacity; /* FIFO capacity in cells (0 = sized from the domain) */
+} vf_fluid_desc;
+
+/* A voxel edit or a voxel change: absolute coordinates + material. */
+typedef struct vf_voxel {
+  int32_t x, y, z;
+  uint8_t m;
+  uint8_t pad[3];
+} vf_voxel;
+
+typedef struct vf_fluid_stats {
+  uint64_t tick_no;            /* FluidSim::tick_no */
+  uint64_t last_tick_cells;    /* FluidSim::last_tick_cells (src/fluid.rs:271-273) */
+  uint64_t active_count;       /* FluidSim::active_count (:262-264) */
+  uint64_t partial_count;      /* FluidSim::partial_count (:268-270) */
+  uint64_t seed_count;         /* level seeds pending */
+  uint64_t level_round;        /* a levelling round is open */
+  uint64_t last_level_cells;   /* cells levelled in the last levelling pass */
+  uint64_t memory_bytes;       /* device bytes held by this handle (FluidSim::memory_bytes) */
+  uint64_t cells_total;        /* sum of last_tick_cells over all ticks */
+  uint64_t pull_attempts;      /* pressure pulls attempted, all ticks */
+  uint64_t pull_success;       /* pressure pulls that moved water */
+  uint64_t bfs_visits;         /* pressure-BFS queue entries examined */
+  uint64_t level_cells_total;  /* cells gathered by level flood fills */
+  uint64_t atlas_used;         /* device bricks materialised */
+  uint64_t changes_pending;    /* voxel changes not yet downloaded */
+} vf_fluid_stats;
+
+/* FluidSim::default(). */
+int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out);
+void vf_fluid_destroy(vf_fluid* h);
+const char* vf_fluid_last_error(const vf_fluid* h);
+
+/* Mirror the host world onto the device (grid u32 per brick in the reference encoding, bricks
+ * 512 bytes each, ring slots as (cx, cz, loaded) triples when ring_w > 0). Replaces any world
+ * uploaded before; the fluid state (queue, partials) is kept. */
+int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32_t bricks_x, int32_t bricks_y,
+                          int32_t bricks_z, const uint32_t* grid, const uint8_t* bricks, uint64_t nbricks,
+                          int32_t ring_w, const int32_t* ring_slots);
+
+/* Host voxel writes made outside the fluid (brush, undo, paste) mirrored to the device; call
+ * before the next tick. */
+int vf_fluid_apply_voxel_edits(vf_fluid* h, const vf_voxel* edits, uint64_t n);
+
+/* FluidSim::wake (src/fluid.rs:358-366), box inclusive. */
+int vf_fluid_wake(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1);
+/* FluidSim::displace (src/fluid.rs:370-408). */
+int vf_fluid_displace(vf_fluid* h, int32_t x, int32_t y, int32_t z);
+/* apply_brush with displace as its on_water hook (src/edit/brush.rs:93-111,
+ * src/app/scene_edit.rs:231-232): for each cell in order, carve (m = 0) clears solid voxels,
+ * place (m != 0) fills air/water voxels, displacing water first. *n_changed = voxels written. */
+int vf_fluid_apply_brush(vf_fluid* h, const int32_t* xyz, uint64_t n, uint8_t m, uint64_t* n_changed);
+/* Rain emitter (harness edit): for each cell, vol' = min(1, vol + amount) through set_volume,
+ * then wake the cell. */
+int vf_fluid_emit(vf_fluid* h, const int32_t* xyz, uint64_t n, float amount);
+/* FluidSim::set_partial (src/fluid.rs:278-282). */
+int vf_fluid_set_partial(vf_fluid* h, int32_t x, int32_t y, int32_t z, float v);
+
+/* FluidSim::tick (src/fluid.rs:564-657), n_ticks times back to back on the device.
+ * *changed (optional) = 1 if any voxel changed. */
+int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed);
+/* FluidSim::update (src/fluid.rs:662-676): fixed 20 Hz, at most 3 ticks per call. */
+int vf_fluid_update(vf_fluid* h, float dt, int32_t* changed);
+
+/* Voxel changes since the last download (final material per changed voxel, any order).
+ * Writes at most cap entries, sets *n to the total pending; entries not copied stay pending. */
+int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n);
+
+/* FluidSim::volume (src/fluid.rs:251-260). */
+int vf_fluid_volume(vf_fluid* h, int32_t x, int32_t y, int32_t z, float* out);
+/* FluidSim::idle (:265-267). */
+int vf_fluid_idle(vf_fluid* h, int32_t* out);
+int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* out);
+
+/* FluidSim::partials().for_each (src/fluid.rs:165-175): every partial cell as (x,y,z) + volume,
+ * in ascending (page, local index) order. Writes at most cap, *n = total. */
+int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap, uint64_t* n);
+/* FluidSim::shift (src/fluid.rs:696-720): floating origin moved by (dx, dz) voxels. */
+int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz);
+/* FluidSim::reset (src/fluid.rs:318-320): the fluid state only; the world mirror stays. */
+int vf_fluid_reset(vf_fluid* h);
+
+/* Differential-test snapshot: the FIFO (x,y,z triples, oldest first) and the level seed list
+ * (bottom to top). Writes at most cap of each; *nq / *ns = lengths. */
+int vf_fluid_snapshot_queue(vf_fluid* h, int32_t* q_xyz, uint64_t q_cap, uint64_t* nq, int32_t* s_xyz, uint64_t s_cap, uint64_t* ns);
+/* Dense export of a box: materials and partial volumes (0 = no partial entry), index
+ * ((z-z0)*sy + (y-y0))*sx + (x-x0). */
+int vf_fluid_export_box(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t sx, int32_t sy, int32_t sz, uint8_t* mat, float* part);
+/* Order-independent digests, computed on the device, of the voxel+partial state and of the
+ * FIFO and seed list (same definitions as the test oracle's). */
+int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* seeds);
+
+/* ---- batched regions: pattern (2) of the engine. Every handle is an independent FluidSim
+ * (its own world, FIFO, caps); one launch steps all of them n_ticks times, one CTA per region.
+ * All handles must live on the same device; the launch runs on hs[0]'s stream. */
+int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,42 @@
+"""The C-ABI library loads and exports every symbol its headers declare (no GPU needed)."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    names = set()
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"\b(vf_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_headers_declare_entry_points():
+    names = declared_symbols()
+    for n in ("vf_fluid_create", "vf_fluid_tick", "vf_fluid_upload_world", "vf_fluid_download_changes", "vf_world_create"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(built):
+    lib = ctypes.CDLL(str(ROOT / "voxelforge-rustrewrite_b200" / "libvf_fluid.so"))
+    missing = [n for n in sorted(declared_symbols()) if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_no_device_fails_loudly(vf):
+    """Without a usable CUDA device the fluid refuses to run (no CPU fallback)."""
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    w = vf.World(16, 16, 16)
+    try:
+        vf.FluidSim(w)
+    except vf.VfError as e:
+        assert e.code == -6
+    else:
+        raise AssertionError("FluidSim ran without a CUDA device")

@@ -1,0 +1,206 @@
+"""Bit-exact parity of the CUDA engine (through the C ABI) against the oracle, after every tick.
+
+Bar: materials and f32 partial volumes bit-identical, FIFO and level-seed list identical in
+order, on every tick (src/fluid.rs semantics). Sizes are scaled so the oracle finishes in
+seconds; full sizes are covered by the digest tests.
+"""
+import numpy as np
+import pytest
+
+from conftest import assert_same_digest, assert_same_state, oracle_for
+
+pytestmark = pytest.mark.gpu
+STONE, WATER = 3, 5
+
+
+def pair(vf, orc, world):
+    o = oracle_for(orc, world)
+    sim = vf.FluidSim(world, device=0)
+    return sim, o
+
+
+def test_basin_300_ticks_bit_exact(vf, orc):
+    """Workload 1 (64^3 basin): full state + FIFO every tick for 300 ticks."""
+    wl = vf.Workload(1)
+    sim, o = pair(vf, orc, wl.world(0))
+    for box in wl.wakes(0):
+        sim.wake(*map(int, box))
+        o.wake(*map(int, box))
+    for t in range(1, 301):
+        ch_g = sim.tick()
+        ch_o = o.tick()
+        assert ch_g == ch_o, f"changed flag differs at tick {t}"
+        if t <= 40 or t % 10 == 0:
+            assert_same_state(sim, o, (-1, 0, -1, 66, 65, 66), t)
+        else:
+            assert_same_digest(sim, o, t)
+        assert sim.last_tick_cells() == o.last_tick_cells()
+    assert sim.partial_count() == o.partial_count()
+
+
+def basin(vf):
+    w = vf.World(64, 32, 64)
+    w.fill_box(0, 0, 0, 63, 3, 63, STONE)
+    w.fill_box(0, 4, 0, 63, 31, 0, STONE)
+    w.fill_box(0, 4, 63, 63, 31, 63, STONE)
+    w.fill_box(0, 4, 0, 0, 31, 63, STONE)
+    w.fill_box(63, 4, 0, 63, 31, 63, STONE)
+    return w
+
+
+def test_column_falls_spreads_and_conserves_volume(vf, orc):  # src/fluid.rs:752-771
+    w = basin(vf)
+    w.fill_box(30, 10, 30, 33, 25, 33, WATER)
+    sim, o = pair(vf, orc, w)
+    sim.wake(29, 9, 29, 34, 26, 34)
+    o.wake(29, 9, 29, 34, 26, 34)
+    before = o.total(0, 0, 0, 64, 32, 64)
+    for t in range(1, 2001):
+        sim.tick()
+        o.tick()
+        assert_same_digest(sim, o, t)
+        if o.idle():
+            assert sim.idle()
+            break
+    assert_same_state(sim, o, (-1, 0, -1, 66, 33, 66))
+    m, p = sim.export_box(0, 0, 0, 64, 32, 64)
+    vol = np.where(p > 0, p, (m == WATER).astype(np.float32)).astype(np.float64)
+    after = vol.sum()
+    assert abs(before - after) < 0.05 * before
+    assert vol[:, 6:, :].sum() < 1.0
+    assert sim.volume(10, 4, 10) > 0.0 or sim.volume(50, 4, 50) > 0.0
+
+
+def test_displace_moves_water_up(vf, orc):  # src/fluid.rs:773-782
+    w = basin(vf)
+    w.fill_box(1, 4, 1, 62, 5, 62, WATER)
+    sim, o = pair(vf, orc, w)
+    sim.displace(20, 4, 20)
+    sim.apply_voxel_edits([(20, 4, 20, STONE)])
+    o.displace(20, 4, 20)
+    o.set_voxel(20, 4, 20, STONE)
+    m, _ = sim.export_box(20, 6, 20, 1, 1, 1)
+    assert m[0, 0, 0] == WATER
+    assert not sim.idle()
+    assert_same_state(sim, o, (-1, 0, -1, 66, 33, 66))
+
+
+def test_hole_under_a_lake_drains_it_level(vf, orc):  # src/fluid.rs:800-817
+    w = basin(vf)
+    w.fill_box(1, 4, 1, 62, 7, 62, WATER)
+    w.fill_box(1, 1, 1, 20, 2, 20, 0)
+    w.set_voxel(10, 3, 10, 0)
+    sim, o = pair(vf, orc, w)
+    sim.wake(9, 2, 9, 11, 5, 11)
+    o.wake(9, 2, 9, 11, 5, 11)
+    for t in range(1, 401):
+        sim.tick()
+        o.tick()
+        if t % 20 == 0:
+            assert_same_digest(sim, o, t)
+    assert_same_state(sim, o, (-1, 0, -1, 66, 33, 66), 400)
+    assert sim.volume(5, 1, 5) > 0.5
+    assert abs(sim.volume(12, 7, 10) - sim.volume(50, 7, 50)) < 0.2
+
+
+@pytest.mark.parametrize("wid,scale,ticks", [(2, 0.125, 120), (3, 0.05, 80), (4, 0.12, 60), (5, 0.05, 60)])
+def test_workloads_scaled_every_tick(vf, orc, wid, scale, ticks):
+    """Scaled dam break / regions / ring + rain / regions + sphere edits: digest every tick."""
+    wl = vf.Workload(wid, scale, 1)
+    for r in range(wl.regions):
+        sim, o = pair(vf, orc, wl.world(r))
+        for box in wl.wakes(r):
+            sim.wake(*map(int, box))
+            o.wake(*map(int, box))
+        em, amt = wl.emitters(r)
+        for t in range(ticks):
+            if wl.emit_every and t % wl.emit_every == 0 and len(em):
+                sim.emit(em, amt)
+                o.emit(em, amt)
+            ed = wl.edit(r, t)
+            if ed is not None:
+                cells, m, wake = ed
+                n_g = sim.apply_brush(cells, m)
+                n_o = o.apply_brush(cells, m)
+                assert n_g == n_o
+                sim.wake(*map(int, wake))
+                o.wake(*map(int, wake))
+            sim.tick()
+            o.tick()
+            assert_same_digest(sim, o, t + 1)
+            assert sim.last_tick_cells() == o.last_tick_cells()
+        sim.close()
+
+
+def test_batched_regions_match_individual_oracles(vf, orc):
+    """One launch over many regions (one CTA each) equals each region's own oracle."""
+    wl = vf.Workload(3, 0.08, 7)
+    sims, oracles = [], []
+    for r in range(wl.regions):
+        sim, o = pair(vf, orc, wl.world(r))
+        for box in wl.wakes(r):
+            sim.wake(*map(int, box))
+            o.wake(*map(int, box))
+        sims.append(sim)
+        oracles.append(o)
+    for step in range(4):
+        vf.batch_tick(sims, 10)
+        for o in oracles:
+            o.tick(10)
+        for r, (s, o) in enumerate(zip(sims, oracles)):
+            assert_same_digest(s, o, (step + 1) * 10)
+
+
+def test_download_changes_keeps_host_world_coherent(vf, orc):
+    wl = vf.Workload(1)
+    w = wl.world(0)
+    sim, o = pair(vf, orc, w)
+    for box in wl.wakes(0):
+        sim.wake(*map(int, box))
+        o.wake(*map(int, box))
+    for _ in range(5):
+        sim.tick(10)
+        o.tick(10)
+        sim.sync_world()
+    om, _ = o.export_box(0, 0, 0, 64, 64, 64)
+    hm = np.array([[[w.get_voxel(x, y, z) for x in range(64)] for y in range(64)] for z in range(64)], np.uint8)
+    assert np.array_equal(hm, om)
+
+
+def test_update_matches_reference_accumulator(vf, orc):
+    wl = vf.Workload(1)
+    sim, o = pair(vf, orc, wl.world(0))
+    for box in wl.wakes(0):
+        sim.wake(*map(int, box))
+        o.wake(*map(int, box))
+    for dt in [0.016, 0.033, 0.1, 0.5, 0.01, 0.2, 0.07, 0.0]:
+        sim.update(dt)
+        o.update(dt)
+        assert sim.stats().tick_no == o.tick_no()
+        assert_same_digest(sim, o)
+
+
+def test_partials_export_and_set_partial(vf, orc):
+    wl = vf.Workload(1)
+    sim, o = pair(vf, orc, wl.world(0))
+    for box in wl.wakes(0):
+        sim.wake(*map(int, box))
+        o.wake(*map(int, box))
+    sim.tick(60)
+    o.tick(60)
+    xyz, vol = sim.partials()
+    assert len(vol) == o.partial_count() == sim.partial_count()
+    for (x, y, z), v in zip(xyz[:200], vol[:200]):
+        assert np.float32(o.volume(int(x), int(y), int(z))) == v
+    # restore into a fresh sim the way saves do (src/app/saves.rs:251-256)
+    sim.reset()
+    o.reset()
+    for (x, y, z), v in zip(xyz, vol):
+        sim.set_partial(int(x), int(y), int(z), float(v))
+        o.set_partial(int(x), int(y), int(z), float(v))
+        sim.wake(int(x), int(y), int(z), int(x), int(y), int(z))
+        o.wake(int(x), int(y), int(z), int(x), int(y), int(z))
+    for t in range(10):
+        sim.tick()
+        o.tick()
+        assert_same_digest(sim, o, t + 1)

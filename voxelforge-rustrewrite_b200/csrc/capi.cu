@@ -1,0 +1,664 @@
+// Host side of the C ABI (include/vf_fluid.h): device memory layout, uploads, launches,
+// downloads. The reference's FluidSim methods map one to one onto vf_fluid_* calls.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/vf_fluid.h"
+#include "kernels.cuh"
+
+using namespace vfe;
+
+struct vf_fluid {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Region R{};
+  Region* dR = nullptr;
+  Ctl* hctl = nullptr;  // pinned mirror
+  bool uploaded = false;
+  std::string err;
+  std::vector<void*> dev_allocs;
+  uint64_t want_atlas = 0, want_queue = 0;
+  int pad = 32;
+  float acc = 0.0f;  // FluidSim::acc (fluid.rs:243), host-side like the reference's
+  // download scratch
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // tick launch shape
+  int smem_bytes = 0;
+};
+
+namespace {
+
+int fail(vf_fluid* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(h, VF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+int dalloc(vf_fluid* h, T** p, size_t count, bool zero = true) {
+  size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) return fail(h, VF_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->dev_allocs.push_back(*p);
+  if (zero) {
+    e = cudaMemsetAsync(*p, 0, bytes, h->stream);
+    if (e != cudaSuccess) return fail(h, VF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return VF_OK;
+}
+
+void free_world(vf_fluid* h) {
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void* p : h->dev_allocs) cudaFree(p);
+  h->dev_allocs.clear();
+  h->dR = nullptr;
+  h->scratch = nullptr;
+  h->scratch_bytes = 0;
+  h->uploaded = false;
+}
+
+int ensure_scratch(vf_fluid* h, size_t bytes) {
+  if (h->scratch_bytes >= bytes) return VF_OK;
+  if (h->scratch) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->scratch);
+    auto it = std::find(h->dev_allocs.begin(), h->dev_allocs.end(), h->scratch);
+    if (it != h->dev_allocs.end()) h->dev_allocs.erase(it);
+  }
+  size_t b = std::max<size_t>(bytes, 1 << 20);
+  cudaError_t e = cudaMalloc(&h->scratch, b);
+  if (e != cudaSuccess) {
+    h->scratch = nullptr;
+    h->scratch_bytes = 0;
+    return fail(h, VF_ERR_OOM, "scratch alloc");
+  }
+  h->dev_allocs.push_back(h->scratch);
+  h->scratch_bytes = b;
+  return VF_OK;
+}
+
+int sync_ctl(vf_fluid* h) {
+  CK(cudaMemcpyAsync(h->hctl, h->R.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->hctl->status != 0) {
+    char b[128];
+    snprintf(b, sizeof b, "device status %d (site %u)", h->hctl->status, h->hctl->err_info);
+    return fail(h, h->hctl->status, b);
+  }
+  return VF_OK;
+}
+
+uint64_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+int check(vf_fluid* h) {
+  if (!h) return VF_ERR_INVALID;
+  if (!h->uploaded) return fail(h, VF_ERR_STATE, "no world uploaded");
+  return VF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
+  if (!out) return VF_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return VF_ERR_NO_DEVICE;
+  auto* h = new vf_fluid();
+  h->device = desc ? desc->device : 0;
+  if (h->device < 0 || h->device >= ndev) {
+    delete h;
+    return VF_ERR_INVALID;
+  }
+  if (cudaSetDevice(h->device) != cudaSuccess) {
+    delete h;
+    return VF_ERR_NO_DEVICE;
+  }
+  if (desc && desc->stream) {
+    h->stream = (cudaStream_t)desc->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return VF_ERR_CUDA;
+    }
+    h->own_stream = true;
+  }
+  if (desc) {
+    h->want_atlas = desc->atlas_bricks;
+    h->want_queue = desc->queue_capacity;
+  }
+  if (cudaMallocHost(&h->hctl, sizeof(Ctl)) != cudaSuccess) {
+    delete h;
+    return VF_ERR_OOM;
+  }
+  std::memset(h->hctl, 0, sizeof(Ctl));
+  // the tick kernel's image must load (sm_100a only): probe its attributes
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_tick) != cudaSuccess) {
+    cudaFreeHost(h->hctl);
+    delete h;
+    return VF_ERR_NO_DEVICE;
+  }
+  h->smem_bytes = (int)sizeof(TickSmem);
+  cudaFuncSetAttribute(k_tick, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_bytes);
+  *out = h;
+  return VF_OK;
+}
+
+void vf_fluid_destroy(vf_fluid* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  free_world(h);
+  if (h->hctl) cudaFreeHost(h->hctl);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* vf_fluid_last_error(const vf_fluid* h) { return h ? h->err.c_str() : "null handle"; }
+
+int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32_t bricks_x, int32_t bricks_y, int32_t bricks_z,
+                          const uint32_t* grid, const uint8_t* bricks, uint64_t nbricks, int32_t ring_w, const int32_t* ring_slots) {
+  if (!h || !grid || nx <= 0 || ny <= 0 || nz <= 0 || bricks_x <= 0 || bricks_y <= 0 || bricks_z <= 0) return VF_ERR_INVALID;
+  if (ring_w && (!ring_slots || (ring_w & (ring_w - 1)))) return VF_ERR_INVALID;
+  if (cudaSetDevice(h->device) != cudaSuccess) return VF_ERR_CUDA;
+  if (h->uploaded) return fail(h, VF_ERR_STATE, "world already uploaded: create a new handle or use apply_voxel_edits");
+  Region R{};
+  R.nx = nx;
+  R.ny = ny;
+  R.nz = nz;
+  R.bx = bricks_x;
+  R.by = bricks_y;
+  R.bz = bricks_z;
+  R.ring_w = ring_w;
+  const int P = h->pad;
+  if (!ring_w) {
+    R.px0 = -P;
+    R.pz0 = -P;
+    R.PX = nx + 2 * P;
+    R.PZ = nz + 2 * P;
+  } else {
+    // bounding box of the loaded chunks (absolute chunk coords)
+    int cx0 = 1 << 30, cx1 = -(1 << 30), cz0 = 1 << 30, cz1 = -(1 << 30);
+    for (int i = 0; i < ring_w * ring_w; ++i)
+      if (ring_slots[3 * i + 2]) {
+        cx0 = std::min(cx0, ring_slots[3 * i]);
+        cx1 = std::max(cx1, ring_slots[3 * i]);
+        cz0 = std::min(cz0, ring_slots[3 * i + 1]);
+        cz1 = std::max(cz1, ring_slots[3 * i + 1]);
+      }
+    if (cx0 > cx1) cx0 = cx1 = cz0 = cz1 = 0;
+    R.px0 = cx0 * 128 - P;
+    R.pz0 = cz0 * 128 - P;
+    R.PX = (cx1 - cx0 + 1) * 128 + 2 * P;
+    R.PZ = (cz1 - cz0 + 1) * 128 + 2 * P;
+  }
+  R.PY = ny + P;
+  uint64_t ncells = (uint64_t)R.PX * R.PY * R.PZ;
+  if (ncells >= 0xFFFFFFF0ull) return fail(h, VF_ERR_RANGE, "domain too large for 32-bit cell ids");
+  R.ncells = (unsigned)ncells;
+  R.TX = (R.PX + 63) / 64;
+  R.TZ = (R.PZ + 63) / 64;
+  const uint64_t nb = (uint64_t)bricks_x * bricks_y * bricks_z;
+  // device grid: detailed host bricks get atlas slots in grid order
+  std::vector<uint32_t> dgrid(nb);
+  uint64_t nd = 0, nfree_uniform = 0;
+  for (uint64_t gi = 0; gi < nb; ++gi) {
+    uint32_t v = grid[gi];
+    if (v >= 256) {
+      if (v - 256 >= nbricks || !bricks) return fail(h, VF_ERR_INVALID, "grid names a brick out of range");
+      dgrid[gi] = 256 + (uint32_t)nd++;
+    } else {
+      dgrid[gi] = v;
+      if (v == 0 || v == VF_FLUID_WATER) ++nfree_uniform;
+    }
+  }
+  uint64_t cap = h->want_atlas ? h->want_atlas : nd + nfree_uniform + 1024;
+  cap = std::max<uint64_t>(cap, nd + 64);
+  if (cap > 0xFFFFFF00ull - 256) return fail(h, VF_ERR_RANGE, "atlas too large");
+  R.atlas_cap = (unsigned)cap;
+  int rc;
+  if ((rc = dalloc(h, &R.grid, nb, false))) return rc;
+  if ((rc = dalloc(h, &R.amat, cap * 512, false))) return rc;
+  if ((rc = dalloc(h, &R.avol, cap * 512, false))) return rc;
+  CK(cudaMemsetAsync(R.avol, 0, nd * 512 * sizeof(float) + 16, h->stream));
+  CK(cudaMemcpyAsync(R.grid, dgrid.data(), nb * 4, cudaMemcpyHostToDevice, h->stream));
+  {
+    std::vector<uint8_t> tmp(std::max<uint64_t>(nd, 1) * 512);
+    uint64_t k = 0;
+    for (uint64_t gi = 0; gi < nb; ++gi)
+      if (grid[gi] >= 256) std::memcpy(&tmp[(k++) * 512], bricks + (uint64_t)(grid[gi] - 256) * 512, 512);
+    CK(cudaMemcpyAsync(R.amat, tmp.data(), nd * 512, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  if ((rc = dalloc(h, &R.ring, std::max(1, 3 * ring_w * ring_w)))) return rc;
+  if (ring_w) CK(cudaMemcpyAsync(R.ring, ring_slots, 3 * ring_w * ring_w * 4, cudaMemcpyHostToDevice, h->stream));
+  const uint64_t words = (ncells + 31) / 32;
+  if ((rc = dalloc(h, &R.active, words))) return rc;
+  if ((rc = dalloc(h, &R.seedbits, words))) return rc;
+  if ((rc = dalloc(h, &R.chgbits, words))) return rc;
+  const uint64_t tiles = (uint64_t)R.TX * R.PY * R.TZ;
+  if ((rc = dalloc(h, &R.marks, tiles * 128))) return rc;
+  if ((rc = dalloc(h, &R.mark_list, tiles))) return rc;
+  if ((rc = dalloc(h, &R.mark_tflag, tiles))) return rc;
+  R.chg_cap = 1u << 22;
+  if ((rc = dalloc(h, &R.chg, R.chg_cap, false))) return rc;
+  uint64_t qcap = next_pow2(std::max<uint64_t>({h->want_queue, std::min<uint64_t>(ncells, 1ull << 22), 1ull << 16}));
+  R.qmask = qcap - 1;
+  if ((rc = dalloc(h, &R.queue, qcap, false))) return rc;
+  if ((rc = dalloc(h, &R.cells, MAX_CELLS_PER_TICK, false))) return rc;
+  if ((rc = dalloc(h, &R.cells_tmp, MAX_CELLS_PER_TICK, false))) return rc;
+  if ((rc = dalloc(h, &R.seeds, MAX_LEVEL_SEEDS, false))) return rc;
+  if ((rc = dalloc(h, &R.lvl_id, MAX_LEVEL_CELLS + 8, false))) return rc;
+  if ((rc = dalloc(h, &R.lvl_vol, MAX_LEVEL_CELLS + 8, false))) return rc;
+  if ((rc = dalloc(h, &R.ctl, 1))) return rc;
+  std::memset(h->hctl, 0, sizeof(Ctl));
+  h->hctl->atlas_used = (unsigned)nd;
+  CK(cudaMemcpyAsync(R.ctl, h->hctl, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  if ((rc = dalloc(h, &h->dR, 1, false))) return rc;
+  CK(cudaMemcpyAsync(h->dR, &R, sizeof(Region), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->R = R;
+  h->uploaded = true;
+  h->acc = 0.0f;
+  return VF_OK;
+}
+
+int vf_fluid_apply_voxel_edits(vf_fluid* h, const vf_voxel* edits, uint64_t n) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (!n) return VF_OK;
+  if (!edits) return VF_ERR_INVALID;
+  if ((rc = ensure_scratch(h, n * 16))) return rc;
+  std::vector<int> q(4 * n);
+  for (uint64_t i = 0; i < n; ++i) {
+    q[4 * i] = edits[i].x;
+    q[4 * i + 1] = edits[i].y;
+    q[4 * i + 2] = edits[i].z;
+    q[4 * i + 3] = edits[i].m;
+  }
+  CK(cudaMemcpyAsync(h->scratch, q.data(), n * 16, cudaMemcpyHostToDevice, h->stream));
+  k_edit<<<1, 32, 0, h->stream>>>(h->R, ED_VOXELS, (const int*)h->scratch, n, 0, 0.0f, nullptr);
+  CK(cudaGetLastError());
+  return sync_ctl(h);
+}
+
+int vf_fluid_wake(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (x1 < x0 || y1 < y0 || z1 < z0) return VF_OK;  // empty box: the reference's loops do nothing
+  y0 = std::max(y0, 0);                            // activate ignores y < 0 (fluid.rs:293)
+  if (y1 < y0) return VF_OK;
+  if (!in_dom(h->R, x0, y0, z0) || !in_dom(h->R, x1, y1, z1)) return fail(h, VF_ERR_RANGE, "wake box outside the padded domain");
+  k_wake_box<<<1, 1024, 0, h->stream>>>(h->R, x0, y0, z0, x1, y1, z1);
+  CK(cudaGetLastError());
+  return sync_ctl(h);
+}
+
+static int run_edit(vf_fluid* h, int kind, const int32_t* xyz, uint64_t n, int m, float amount, uint64_t* out_count, size_t ints_per) {
+  int rc = check(h);
+  if (rc) return rc;
+  size_t bytes = std::max<size_t>(n * ints_per * 4, 16) + 64;
+  if ((rc = ensure_scratch(h, bytes))) return rc;
+  if (n) CK(cudaMemcpyAsync(h->scratch, xyz, n * ints_per * 4, cudaMemcpyHostToDevice, h->stream));
+  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + bytes - 64);
+  k_edit<<<1, 32, 0, h->stream>>>(h->R, kind, (const int*)h->scratch, n, m, amount, out_count ? dcount : nullptr);
+  CK(cudaGetLastError());
+  if (out_count) {
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, dcount, 8, cudaMemcpyDeviceToHost, h->stream));
+    rc = sync_ctl(h);
+    *out_count = c;
+    return rc;
+  }
+  return sync_ctl(h);
+}
+
+int vf_fluid_displace(vf_fluid* h, int32_t x, int32_t y, int32_t z) {
+  int32_t p[3] = {x, y, z};
+  return run_edit(h, ED_DISPLACE, p, 1, 0, 0.0f, nullptr, 3);
+}
+
+int vf_fluid_apply_brush(vf_fluid* h, const int32_t* xyz, uint64_t n, uint8_t m, uint64_t* n_changed) {
+  if (n && !xyz) return VF_ERR_INVALID;
+  uint64_t c = 0;
+  int rc = run_edit(h, ED_BRUSH, xyz, n, m, 0.0f, &c, 3);
+  if (n_changed) *n_changed = c;
+  return rc;
+}
+
+int vf_fluid_emit(vf_fluid* h, const int32_t* xyz, uint64_t n, float amount) {
+  if (n && !xyz) return VF_ERR_INVALID;
+  return run_edit(h, ED_EMIT, xyz, n, 0, amount, nullptr, 3);
+}
+
+int vf_fluid_set_partial(vf_fluid* h, int32_t x, int32_t y, int32_t z, float v) {
+  int32_t p[3] = {x, y, z};
+  return run_edit(h, ED_SET_PARTIAL, p, 1, 0, v, nullptr, 3);
+}
+
+int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (n_ticks < 0) return VF_ERR_INVALID;
+  CK(cudaMemsetAsync(&h->R.ctl->changed, 0, sizeof(unsigned), h->stream));
+  if (n_ticks > 0) {
+    k_tick<<<1, TICK_THREADS, h->smem_bytes, h->stream>>>(h->dR, 1, n_ticks);
+    CK(cudaGetLastError());
+  }
+  rc = sync_ctl(h);
+  if (changed) *changed = h->hctl->changed ? 1 : 0;
+  return rc;
+}
+
+int vf_fluid_idle(vf_fluid* h, int32_t* out) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (out) *out = (h->hctl->qtail == h->hctl->qhead && h->hctl->nseeds == 0) ? 1 : 0;  // fluid.rs:265-267
+  return VF_OK;
+}
+
+int vf_fluid_update(vf_fluid* h, float dt, int32_t* changed) {  // fluid.rs:662-676
+  int32_t idle = 0;
+  int rc = vf_fluid_idle(h, &idle);
+  if (rc) return rc;
+  if (changed) *changed = 0;
+  if (idle) {
+    h->acc = 0.0f;
+    return VF_OK;
+  }
+  const float step = 1.0f / VF_FLUID_TICK_HZ;
+  h->acc = std::min(h->acc + std::min(dt, 0.25f), 3.0f / VF_FLUID_TICK_HZ);
+  int n = 0;
+  while (h->acc >= step && n < 3) {
+    h->acc -= step;
+    n += 1;
+  }
+  if (n == 0) return VF_OK;
+  return vf_fluid_tick(h, n, changed);
+}
+
+int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  uint64_t total = std::min<uint64_t>(h->hctl->nchg, h->R.chg_cap);
+  if (n) *n = total;
+  uint64_t take = std::min(total, cap);
+  if (!take || !out) return VF_OK;
+  if ((rc = ensure_scratch(h, take * sizeof(Voxel)))) return rc;
+  k_gather_changes<<<(unsigned)std::min<uint64_t>((take + 255) / 256, 4096), 256, 0, h->stream>>>(h->R, take, (Voxel*)h->scratch);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, h->scratch, take * sizeof(Voxel), cudaMemcpyDeviceToHost, h->stream));
+  if (take < total) {
+    // keep the rest pending: move it to the front of the list
+    CK(cudaMemcpyAsync(h->R.chg, h->R.chg + take, (total - take) * 4, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  unsigned long long left = total - take;
+  CK(cudaMemcpyAsync(&h->R.ctl->nchg, &left, 8, cudaMemcpyHostToDevice, h->stream));
+  return sync_ctl(h);
+}
+
+int vf_fluid_volume(vf_fluid* h, int32_t x, int32_t y, int32_t z, float* out) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (!out) return VF_ERR_INVALID;
+  if ((rc = ensure_scratch(h, 64))) return rc;
+  k_export_box<<<1, 32, 0, h->stream>>>(h->R, x, y, z, 1, 1, 1, (unsigned char*)h->scratch, (float*)((char*)h->scratch + 16));
+  CK(cudaGetLastError());
+  unsigned char m = 0;
+  float p = 0.0f;
+  CK(cudaMemcpyAsync(&m, h->scratch, 1, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&p, (char*)h->scratch + 16, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  // FluidSim::volume (fluid.rs:251-260); outside cells export as material 0, partial 0
+  *out = p > 0.0f ? p : (m == VF_FLUID_WATER ? 1.0f : 0.0f);
+  return VF_OK;
+}
+
+int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* o) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (!o) return VF_ERR_INVALID;
+  if ((rc = sync_ctl(h))) return rc;
+  const Ctl& c = *h->hctl;
+  std::memset(o, 0, sizeof(*o));
+  o->tick_no = c.tick_no;
+  o->last_tick_cells = c.last_cells;
+  o->active_count = c.qtail - c.qhead;
+  o->partial_count = (uint64_t)c.partial_count;
+  o->seed_count = c.nseeds;
+  o->level_round = c.level_round;
+  o->last_level_cells = c.last_level_cells;
+  size_t bytes = 0;
+  {
+    const Region& R = h->R;
+    uint64_t words = ((uint64_t)R.ncells + 31) / 32;
+    uint64_t tiles = (uint64_t)R.TX * R.PY * R.TZ;
+    bytes += (uint64_t)R.bx * R.by * R.bz * 4 + (uint64_t)R.atlas_cap * 512 * 5 + words * 4 * 3 + tiles * (512 + 8) +
+             (uint64_t)R.chg_cap * 4 + (R.qmask + 1) * 4 + (uint64_t)MAX_CELLS_PER_TICK * 8 + MAX_LEVEL_SEEDS * 4 +
+             (uint64_t)(MAX_LEVEL_CELLS + 8) * 8;
+  }
+  o->memory_bytes = bytes;
+  o->cells_total = c.cells_total;
+  o->pull_attempts = c.pull_attempts;
+  o->pull_success = c.pull_success;
+  o->bfs_visits = c.bfs_visits;
+  o->level_cells_total = c.level_cells_total;
+  o->atlas_used = c.atlas_used;
+  o->changes_pending = c.nchg;
+  return VF_OK;
+}
+
+int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap, uint64_t* n) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  unsigned nslots = std::min(h->hctl->atlas_used, h->R.atlas_cap);
+  size_t need = (size_t)nslots * 4 + 64 + cap * 16;
+  if ((rc = ensure_scratch(h, need))) return rc;
+  int* slot_brick = (int*)h->scratch;
+  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + (size_t)nslots * 4);
+  int* dxyz = (int*)((char*)h->scratch + (size_t)nslots * 4 + 64);
+  float* dvol = (float*)((char*)dxyz + cap * 12);
+  CK(cudaMemsetAsync(slot_brick, 0xFF, (size_t)nslots * 4 + 8, h->stream));
+  CK(cudaMemsetAsync(dcount, 0, 8, h->stream));
+  uint64_t nb = (uint64_t)h->R.bx * h->R.by * h->R.bz;
+  k_slot_map<<<(unsigned)std::min<uint64_t>((nb + 255) / 256, 8192), 256, 0, h->stream>>>(h->R, slot_brick, nslots);
+  if (nslots)
+    k_export_partials<<<(unsigned)std::min<uint64_t>(((uint64_t)nslots * 512 + 255) / 256, 16384), 256, 0, h->stream>>>(h->R, nslots, dxyz, dvol,
+                                                                                                                         cap, dcount, slot_brick);
+  CK(cudaGetLastError());
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, dcount, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (n) *n = cnt;
+  uint64_t take = std::min<uint64_t>(cnt, cap);
+  if (take && xyz) CK(cudaMemcpy(xyz, dxyz, take * 12, cudaMemcpyDeviceToHost));
+  if (take && vol) CK(cudaMemcpy(vol, dvol, take * 4, cudaMemcpyDeviceToHost));
+  // canonical order: by (x, y, z) ascending? keep (slot, voxel) order but make it deterministic
+  if (take && xyz && vol) {
+    std::vector<uint64_t> idx(take);
+    for (uint64_t i = 0; i < take; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+      return std::make_tuple(xyz[3 * a + 2], xyz[3 * a + 1], xyz[3 * a]) < std::make_tuple(xyz[3 * b + 2], xyz[3 * b + 1], xyz[3 * b]);
+    });
+    std::vector<int32_t> x2(take * 3);
+    std::vector<float> v2(take);
+    for (uint64_t i = 0; i < take; ++i) {
+      std::memcpy(&x2[3 * i], &xyz[3 * idx[i]], 12);
+      v2[i] = vol[idx[i]];
+    }
+    std::memcpy(xyz, x2.data(), take * 12);
+    std::memcpy(vol, v2.data(), take * 4);
+  }
+  return VF_OK;
+}
+
+int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz) {  // fluid.rs:696-720
+  int rc = check(h);
+  if (rc) return rc;
+  // Ring worlds move their origin by whole ring periods (sparse_volume.rs:194-203): the brick
+  // slots then stay where they are, only coordinates change. Cell ids are relative to the padded
+  // domain's origin, so moving the origin re-keys the FIFO, seeds and partials at once.
+  const Region& R = h->R;
+  if (!R.ring_w || (dx % (R.ring_w * 128)) != 0 || (dz % (R.ring_w * 128)) != 0)
+    return fail(h, VF_ERR_RANGE, "shift supports ring worlds moved by whole ring periods");
+  if ((rc = sync_ctl(h))) return rc;
+  h->R.px0 -= dx;
+  h->R.pz0 -= dz;
+  // the ring slots' owners move with the origin (the host rebases its SparseVolume alike)
+  std::vector<int32_t> ring(3 * R.ring_w * R.ring_w);
+  CK(cudaMemcpy(ring.data(), R.ring, ring.size() * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < ring.size(); i += 3) {
+    ring[i] -= dx / 128;
+    ring[i + 1] -= dz / 128;
+  }
+  CK(cudaMemcpy(R.ring, ring.data(), ring.size() * 4, cudaMemcpyHostToDevice));
+  // the levelling round starts over (fluid.rs:715-719)
+  const unsigned nt = h->hctl->mark_ntiles;
+  if (nt) {
+    const uint64_t tiles = (uint64_t)R.TX * R.PY * R.TZ;
+    CK(cudaMemsetAsync(R.marks, 0, tiles * 128 * 4, h->stream));
+    CK(cudaMemsetAsync(R.mark_tflag, 0, tiles * 4, h->stream));
+  }
+  unsigned zero = 0;
+  CK(cudaMemcpyAsync(&R.ctl->mark_ntiles, &zero, 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(&R.ctl->level_round, &zero, 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->dR, &h->R, sizeof(Region), cudaMemcpyHostToDevice, h->stream));
+  return sync_ctl(h);
+}
+
+int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
+  int rc = check(h);
+  if (rc) return rc;
+  const Region& R = h->R;
+  if ((rc = sync_ctl(h))) return rc;
+  unsigned used = h->hctl->atlas_used;
+  CK(cudaMemsetAsync(R.avol, 0, (size_t)used * 512 * 4, h->stream));
+  uint64_t words = ((uint64_t)R.ncells + 31) / 32;
+  CK(cudaMemsetAsync(R.active, 0, words * 4, h->stream));
+  CK(cudaMemsetAsync(R.seedbits, 0, words * 4, h->stream));
+  const uint64_t tiles = (uint64_t)R.TX * R.PY * R.TZ;
+  CK(cudaMemsetAsync(R.marks, 0, tiles * 128 * 4, h->stream));
+  CK(cudaMemsetAsync(R.mark_tflag, 0, tiles * 4, h->stream));
+  Ctl c = *h->hctl;
+  Ctl z{};
+  z.atlas_used = c.atlas_used;
+  z.nchg = c.nchg;  // voxel changes still owed to the host
+  CK(cudaMemcpyAsync(R.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  h->acc = 0.0f;
+  return sync_ctl(h);
+}
+
+int vf_fluid_snapshot_queue(vf_fluid* h, int32_t* q_xyz, uint64_t q_cap, uint64_t* nq, int32_t* s_xyz, uint64_t s_cap, uint64_t* ns) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  const Region& R = h->R;
+  uint64_t len = h->hctl->qtail - h->hctl->qhead;
+  if (nq) *nq = len;
+  uint64_t take = std::min(len, q_cap);
+  if (take && q_xyz) {
+    std::vector<uint32_t> ids(take);
+    uint64_t cap = R.qmask + 1, head = h->hctl->qhead & R.qmask;
+    uint64_t first = std::min(take, cap - head);
+    CK(cudaMemcpy(ids.data(), R.queue + head, first * 4, cudaMemcpyDeviceToHost));
+    if (take > first) CK(cudaMemcpy(ids.data() + first, R.queue, (take - first) * 4, cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < take; ++i) dom_xyz(R, ids[i], q_xyz[3 * i], q_xyz[3 * i + 1], q_xyz[3 * i + 2]);
+  }
+  uint64_t sl = h->hctl->nseeds;
+  if (ns) *ns = sl;
+  uint64_t st = std::min(sl, s_cap);
+  if (st && s_xyz) {
+    std::vector<uint32_t> ids(st);
+    CK(cudaMemcpy(ids.data(), R.seeds, st * 4, cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < st; ++i) dom_xyz(R, ids[i], s_xyz[3 * i], s_xyz[3 * i + 1], s_xyz[3 * i + 2]);
+  }
+  return VF_OK;
+}
+
+int vf_fluid_export_box(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t sx, int32_t sy, int32_t sz, uint8_t* mat, float* part) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (sx <= 0 || sy <= 0 || sz <= 0) return VF_ERR_INVALID;
+  uint64_t n = (uint64_t)sx * sy * sz;
+  if ((rc = ensure_scratch(h, n * 5 + 64))) return rc;
+  unsigned char* dm = (unsigned char*)h->scratch;
+  float* dp = (float*)((char*)h->scratch + ((n + 15) / 16) * 16);
+  k_export_box<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 16384), 256, 0, h->stream>>>(h->R, x0, y0, z0, sx, sy, sz, dm, dp);
+  CK(cudaGetLastError());
+  if (mat) CK(cudaMemcpyAsync(mat, dm, n, cudaMemcpyDeviceToHost, h->stream));
+  if (part) CK(cudaMemcpyAsync(part, dp, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return VF_OK;
+}
+
+int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* seeds) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if ((rc = ensure_scratch(h, 64))) return rc;
+  unsigned long long* d = (unsigned long long*)h->scratch;
+  CK(cudaMemsetAsync(d, 0, 24, h->stream));
+  const Region& R = h->R;
+  uint64_t nvox = (uint64_t)R.bx * R.by * R.bz * 512;
+  k_state_digest<<<(unsigned)std::min<uint64_t>((nvox + 255) / 256, 16384), 256, 0, h->stream>>>(R, d);
+  uint64_t ql = h->hctl->qtail - h->hctl->qhead;
+  if (ql) k_list_digest<<<(unsigned)std::min<uint64_t>((ql + 255) / 256, 4096), 256, 0, h->stream>>>(R, R.queue, ql, h->hctl->qhead, R.qmask, d + 1);
+  uint64_t sl = h->hctl->nseeds;
+  if (sl) k_list_digest<<<(unsigned)((sl + 255) / 256), 256, 0, h->stream>>>(R, R.seeds, sl, 0, 0xFFFFFFFFFFFFFFFFull, d + 2);
+  CK(cudaGetLastError());
+  unsigned long long out[3];
+  CK(cudaMemcpyAsync(out, d, 24, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (state) *state = out[0];
+  if (queue) *queue = out[1];
+  if (seeds) *seeds = out[2];
+  return VF_OK;
+}
+
+// ------------------------------------------------------------------------ batched regions
+int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks) {
+  if (!hs || n <= 0 || n_ticks < 0) return VF_ERR_INVALID;
+  vf_fluid* h = hs[0];
+  for (int i = 0; i < n; ++i) {
+    int rc = check(hs[i]);
+    if (rc) return rc;
+    if (hs[i]->device != h->device) return fail(h, VF_ERR_INVALID, "batched handles must share a device");
+  }
+  std::vector<Region> regs(n);
+  for (int i = 0; i < n; ++i) regs[i] = hs[i]->R;
+  int rc;
+  if ((rc = ensure_scratch(h, sizeof(Region) * n))) return rc;
+  CK(cudaMemcpyAsync(h->scratch, regs.data(), sizeof(Region) * n, cudaMemcpyHostToDevice, h->stream));
+  for (int i = 0; i < n; ++i) CK(cudaMemsetAsync(&regs[i].ctl->changed, 0, 4, h->stream));
+  if (n_ticks) {
+    k_tick<<<n, TICK_THREADS, h->smem_bytes, h->stream>>>((Region*)h->scratch, n, n_ticks);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < n; ++i) {
+    if ((rc = sync_ctl(hs[i]))) return rc;
+  }
+  return VF_OK;
+}
+
+}  // extern "C"

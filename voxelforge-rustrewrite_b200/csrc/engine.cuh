@@ -1,0 +1,167 @@
+// Device data structures and per-cell rules of the CA-water engine (sm_100a).
+//
+// Semantics restate the reference's FluidSim (src/fluid.rs:230-721); every function cites the
+// lines it follows. Layout:
+//   * world mirror: grid u32 per 8^3 brick in the reference's encoding (sparse_volume.rs:3-6)
+//     where a detailed brick's value is 256 + a slot of the device atlas; the atlas holds
+//     materials (u8[512]) and partial volumes (f32[512], 0 = no partial entry, fluid.rs:64-79)
+//     per slot, both with the reference's voxel index lz*64 + ly*8 + lx (== PartialField's
+//     local index x | y<<3 | z<<6). Uniform bricks stay grid values until the fluid writes them.
+//   * scheduler sets (active, level seeds, layer marks, changed voxels) are dense bitmaps over a
+//     padded cell domain; the FIFO is a ring of u32 cell ids of that domain.
+//
+// Floating point: compiled with -fmad=false and no fast-math; f32 where fluid.rs uses f32 and f64
+// where it uses f64, so every result is bit-identical to the reference's sequential sweep.
+#pragma once
+#include <cstdint>
+
+namespace vfe {
+
+constexpr uint8_t WATER = 5;
+constexpr float SHOW_AT = 0.5f;
+constexpr float HIDE_BELOW = 0.3f;
+constexpr float EVAPORATE = 1e-4f;
+constexpr float MIN_SPREAD = 0.05f;
+constexpr float MIN_FLOW = 1e-4f;
+constexpr float SLEEP = 1e-3f;
+constexpr uint32_t MAX_CELLS_PER_TICK = 50000;
+constexpr uint32_t LEVEL_TICKS = 10;
+constexpr uint32_t MAX_LEVEL_CELLS = 400000;
+constexpr uint32_t PRESSURE_SEARCH = 512;
+constexpr uint32_t MAX_PULLS_PER_TICK = 4096;
+constexpr uint32_t LEVEL_BUDGET = 40000;
+constexpr uint32_t MAX_LEVEL_SEEDS = 4096;
+constexpr uint32_t NOSLOT = 0xFFFFFFFFu;
+// Press-BFS queue bound: 5 start cells + 5 pushes per examined entry, 512 entries examined.
+constexpr uint32_t PRESS_QCAP = 5 + 5 * PRESSURE_SEARCH + 8;
+constexpr uint32_t VIS_CAP = 8192;  // smem visited hash (load <= 32%)
+
+// status codes written to Ctl::status by device code (mirrors VF_ERR_*)
+constexpr int ST_OK = 0;
+constexpr int ST_OOM = -2;
+constexpr int ST_TIMEOUT = -4;
+constexpr int ST_RANGE = -5;
+
+struct Ctl {
+  unsigned long long qhead, qtail;  // FIFO positions (monotonic)
+  unsigned long long cells_total, pull_attempts, pull_success, bfs_visits, level_cells_total, activations;
+  long long partial_count;
+  unsigned long long nchg;          // changed voxels pending download
+  unsigned int tick_no, level_round, nseeds, atlas_used;
+  unsigned int last_cells, last_level_cells, changed, mark_ntiles;
+  int status;
+  unsigned int err_info;
+  unsigned int pad[2];
+};
+
+struct Region {
+  // ---- geometry (voxel dims, brick dims, ring width; padded scheduler domain)
+  int nx, ny, nz, bx, by, bz, ring_w;
+  int px0, pz0, PX, PY, PZ;  // domain: x in [px0, px0+PX), y in [0, PY), z in [pz0, pz0+PZ)
+  int TX, TZ;                // layer-mark tiles (64x64) per row / column
+  unsigned int ncells;       // PX*PY*PZ
+  // ---- world mirror
+  unsigned int* grid;        // bx*by*bz
+  unsigned char* amat;       // atlas materials [atlas_cap][512]
+  float* avol;               // atlas partial volumes [atlas_cap][512]
+  unsigned int atlas_cap;
+  int* ring;                 // ring_w*ring_w triples (cx, cz, loaded)
+  // ---- scheduler
+  unsigned int* active;      // ncells bits
+  unsigned int* seedbits;    // ncells bits
+  unsigned int* marks;       // tiles * 128 words
+  unsigned int* mark_list;   // touched tiles
+  unsigned int* mark_tflag;  // per tile: listed in mark_list
+  unsigned int* chgbits;     // ncells bits
+  unsigned int* chg;         // changed ids (chg_cap)
+  unsigned int chg_cap;
+  unsigned int* queue;       // FIFO ring
+  unsigned long long qmask;  // capacity - 1 (power of two)
+  unsigned int* cells;       // drained cells (sort keys), MAX_CELLS_PER_TICK
+  unsigned int* cells_tmp;
+  unsigned int* seeds;       // MAX_LEVEL_SEEDS
+  unsigned int* lvl_id;      // MAX_LEVEL_CELLS + 8
+  float* lvl_vol;
+  Ctl* ctl;
+};
+
+// ---------------------------------------------------------------- reference key (fluid.rs:46-62)
+__host__ __device__ inline unsigned long long ref_key(int x, int y, int z) {
+  auto f = [](int v) { return (unsigned long long)(((unsigned)v + (1u << 20)) & 0x1FFFFFu); };
+  return f(x) | f(y) << 21 | f(z) << 42;
+}
+
+__host__ __device__ inline unsigned long long fmix64(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+// ------------------------------------------------------------------------ domain ids
+__host__ __device__ inline bool in_dom(const Region& R, int x, int y, int z) {
+  return (unsigned)(x - R.px0) < (unsigned)R.PX && (unsigned)y < (unsigned)R.PY && (unsigned)(z - R.pz0) < (unsigned)R.PZ;
+}
+__host__ __device__ inline unsigned dom_id(const Region& R, int x, int y, int z) {
+  return ((unsigned)(z - R.pz0) * (unsigned)R.PY + (unsigned)y) * (unsigned)R.PX + (unsigned)(x - R.px0);
+}
+__host__ __device__ inline void dom_xyz(const Region& R, unsigned id, int& x, int& y, int& z) {
+  unsigned t = id / (unsigned)R.PX;
+  x = (int)(id - t * (unsigned)R.PX) + R.px0;
+  unsigned zz = t / (unsigned)R.PY;
+  y = (int)(t - zz * (unsigned)R.PY);
+  z = (int)zz + R.pz0;
+}
+// Sort key realising the reference's order (fluid.rs:575-580): (y, z, x), or (y, -z, -x) when
+// the tick number is odd. Unique per cell, < ncells.
+__host__ __device__ inline unsigned sort_key(const Region& R, unsigned id, bool flip) {
+  int x, y, z;
+  dom_xyz(R, id, x, y, z);
+  unsigned xr = (unsigned)(x - R.px0), zr = (unsigned)(z - R.pz0);
+  if (flip) {
+    xr = (unsigned)R.PX - 1u - xr;
+    zr = (unsigned)R.PZ - 1u - zr;
+  }
+  return ((unsigned)y * (unsigned)R.PZ + zr) * (unsigned)R.PX + xr;
+}
+__host__ __device__ inline unsigned key_to_id(const Region& R, unsigned key, bool flip) {
+  unsigned t = key / (unsigned)R.PX;
+  unsigned xr = key - t * (unsigned)R.PX;
+  unsigned y = t / (unsigned)R.PZ;
+  unsigned zr = t - y * (unsigned)R.PZ;
+  if (flip) {
+    xr = (unsigned)R.PX - 1u - xr;
+    zr = (unsigned)R.PZ - 1u - zr;
+  }
+  return (zr * (unsigned)R.PY + y) * (unsigned)R.PX + xr;
+}
+
+// ------------------------------------------------------------------ world access
+// SparseVolume::grid_index (sparse_volume.rs:142-148).
+__host__ __device__ inline unsigned grid_index(const Region& R, int ix, int iy, int iz) {
+  if (R.ring_w) {
+    ix &= R.bx - 1;
+    iz &= R.bz - 1;
+  }
+  return ((unsigned)iz * (unsigned)R.by + (unsigned)iy) * (unsigned)R.bx + (unsigned)ix;
+}
+
+// One cell as the rules see it.
+struct CD {
+  float part;       // partial volume (0 = none)
+  unsigned slot;    // atlas slot of the brick, NOSLOT when the brick is a uniform grid value
+  unsigned gi;      // grid index
+  unsigned char mat;
+  bool out;         // fluid.rs `outside` (:212-217)
+};
+
+__device__ inline bool cd_solid(const CD& c) { return c.out || (c.mat != 0 && c.mat != WATER); }  // fluid.rs:220-226
+__device__ inline float cd_volume(const CD& c) {  // fluid.rs:251-260
+  if (c.out) return 0.0f;
+  if (c.part > 0.0f) return c.part;
+  return c.mat == WATER ? 1.0f : 0.0f;
+}
+
+}  // namespace vfe

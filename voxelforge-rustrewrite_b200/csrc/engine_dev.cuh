@@ -1,0 +1,737 @@
+// Warp-cooperative device implementation of the reference's fluid tick (src/fluid.rs:292-657).
+//
+// One warp owns one region's sweep: it walks the drained cells in the reference's sorted order,
+// so every cell sees exactly the state the sequential Rust loop would show it. Parallelism inside
+// a cell comes from the 32 lanes: the 7-cell footprint, the 6-cell pressure-BFS neighbourhoods and
+// the 12 cells of four level-fill membership tests load in one round each; activations are
+// deduplicated and appended to the FIFO in program order with ballots; bricks are materialised
+// cooperatively. Batching across regions runs one CTA per region (see engine.cu).
+#pragma once
+#include "engine.cuh"
+
+namespace vfe {
+
+constexpr unsigned FULLMASK = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// f32 constant 1.0 - 1e-4 folded in f32 (fluid.rs:323, :337, :513, :594).
+__device__ __forceinline__ float full_level() { return __fsub_rn(1.0f, 1e-4f); }
+
+// ---------------------------------------------------------------------------- world reads
+__device__ __forceinline__ bool chunk_loaded(const Region& R, const int* ring, int cx, int cz) {  // sparse_volume.rs:164-170
+  int m = R.ring_w - 1;
+  int i = ((cz & m) * R.ring_w + (cx & m)) * 3;
+  return ring[i + 2] != 0 && ring[i] == cx && ring[i + 1] == cz;
+}
+
+__device__ __forceinline__ bool outside(const Region& R, const int* ring, int x, int y, int z) {  // fluid.rs:212-217
+  if (y < 0 || y >= R.ny) return true;
+  if (R.ring_w) return !chunk_loaded(R, ring, x >> 7, z >> 7);
+  return x < 0 || z < 0 || x >= R.nx || z >= R.nz;
+}
+
+__device__ __forceinline__ unsigned local_index(int x, int y, int z) { return ((unsigned)(z & 7) << 6) | ((unsigned)(y & 7) << 3) | (unsigned)(x & 7); }
+
+__device__ __forceinline__ CD load_cell(const Region& R, const int* ring, int x, int y, int z) {
+  CD c;
+  c.part = 0.0f;
+  c.slot = NOSLOT;
+  c.gi = 0;
+  c.mat = 0;
+  c.out = outside(R, ring, x, y, z);
+  if (c.out) return c;
+  c.gi = grid_index(R, x >> 3, y >> 3, z >> 3);
+  unsigned g = R.grid[c.gi];
+  if (g < 256u) {
+    c.mat = (unsigned char)g;
+    return c;
+  }
+  c.slot = g - 256u;
+  size_t o = (size_t)c.slot * 512u + local_index(x, y, z);
+  c.mat = R.amat[o];
+  c.part = R.avol[o];
+  return c;
+}
+
+__device__ __forceinline__ CD shfl_cd(const CD& c, int src) {
+  CD r;
+  r.part = __shfl_sync(FULLMASK, c.part, src);
+  r.slot = __shfl_sync(FULLMASK, c.slot, src);
+  r.gi = __shfl_sync(FULLMASK, c.gi, src);
+  unsigned p = __shfl_sync(FULLMASK, (unsigned)c.mat | ((unsigned)c.out << 8), src);
+  r.mat = (unsigned char)(p & 255u);
+  r.out = (p >> 8) != 0;
+  return r;
+}
+
+// Warp-uniform state of one region's sweep.
+struct WS {
+  unsigned long long qhead, qtail;
+  unsigned long long activations, pull_attempts, pull_success, bfs_visits, level_cells_total;
+  long long pdelta;        // partial_count delta (lane-local, reduced at the end)
+  unsigned nseeds;
+  unsigned pulls;          // this tick's pull attempts (fluid.rs:583)
+  unsigned llc;            // last_level_cells
+  unsigned epoch;          // press-BFS visited epoch
+  bool level_round;
+  bool changed;
+};
+
+struct Smem {
+  unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
+  unsigned* pq;             // PRESS_QCAP
+  const int* ring;
+};
+
+__device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
+  if (atomicCAS(&R.ctl->status, 0, st) == 0) R.ctl->err_info = info;
+}
+
+// ---------------------------------------------------------------------- materialisation
+// Bricks that are uniform grid values get an atlas slot before their first write (the
+// reference's SparseVolume::materialize, sparse_volume.rs:250-266; partial pages, fluid.rs:108-128).
+// Lanes with `need` name a grid index; one leader per distinct index allocates, the warp fills.
+__device__ void materialize_lanes(const Region& R, bool need, unsigned gi, unsigned& slot) {
+  const unsigned lane = lane_id();
+  unsigned key = need ? gi : (0xFFFFFFFFu - lane);
+  unsigned peers = __match_any_sync(FULLMASK, key);
+  bool leader = need && !(peers & lanemask_lt());
+  unsigned lead_mask = __ballot_sync(FULLMASK, leader);
+  if (!lead_mask) return;
+  unsigned s = NOSLOT;
+  unsigned g = 0;
+  if (leader) {
+    g = R.grid[gi];
+    if (g >= 256u) {
+      s = g - 256u;
+    } else {
+      s = atomicAdd(&R.ctl->atlas_used, 1u);
+      if (s >= R.atlas_cap) {
+        set_status(R, ST_OOM, 1);
+        s = NOSLOT;
+      }
+    }
+  }
+  // cooperative fill of each new slot
+  for (unsigned m = lead_mask; m; m &= m - 1) {
+    int l = __ffs(m) - 1;
+    unsigned sl = __shfl_sync(FULLMASK, s, l);
+    unsigned gv = __shfl_sync(FULLMASK, g, l);
+    if (sl != NOSLOT && gv < 256u) {
+      unsigned fill = gv & 255u;
+      fill |= fill << 8;
+      fill |= fill << 16;
+      uint4 f4 = make_uint4(fill, fill, fill, fill);
+      reinterpret_cast<uint4*>(R.amat + (size_t)sl * 512u)[lane] = f4;
+      uint4 z4 = make_uint4(0, 0, 0, 0);
+      uint4* vv = reinterpret_cast<uint4*>(R.avol + (size_t)sl * 512u);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vv[lane + 32 * k] = z4;
+    }
+  }
+  __syncwarp();
+  if (leader && s != NOSLOT && g < 256u) R.grid[gi] = 256u + s;
+  int src = need ? (__ffs(peers) - 1) : (int)lane;
+  unsigned s2 = __shfl_sync(FULLMASK, s, src);
+  if (need) slot = s2;
+  __syncwarp();
+}
+
+// --------------------------------------------------------------------------- writes
+__device__ __forceinline__ void record_change(const Region& R, unsigned id) {
+  unsigned old = atomicOr(&R.chgbits[id >> 5], 1u << (id & 31));
+  if (!(old & (1u << (id & 31)))) {
+    unsigned long long i = atomicAdd(&R.ctl->nchg, 1ull);
+    if (i < R.chg_cap) R.chg[i] = id;
+    else set_status(R, ST_OOM, 2);
+  }
+}
+
+__device__ __forceinline__ void write_mat(const Region& R, CD& c, unsigned l, unsigned id, unsigned char m) {
+  if (c.slot == NOSLOT) return;  // materialisation failed (status already set)
+  R.amat[(size_t)c.slot * 512u + l] = m;
+  c.mat = m;
+  record_change(R, id);
+}
+
+__device__ __forceinline__ void erase_part(const Region& R, CD& c, unsigned l, long long& pdelta) {
+  if (c.slot != NOSLOT && c.part > 0.0f) {
+    R.avol[(size_t)c.slot * 512u + l] = 0.0f;
+    c.part = 0.0f;
+    pdelta -= 1;
+  }
+}
+
+// Does set_volume(c, vol) write into the brick (so a uniform brick needs a slot first)?
+__device__ __forceinline__ bool set_volume_needs_slot(const CD& c, float vol) {
+  if (c.slot != NOSLOT) return false;
+  bool is_water = c.mat == WATER;
+  if (vol <= 1e-6f) return is_water;
+  if (vol >= full_level()) return !is_water;
+  return true;
+}
+
+// FluidSim::set_volume (fluid.rs:327-355) on one lane's cell; c.slot must be valid when
+// set_volume_needs_slot said so. Returns "the voxel changed".
+__device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, unsigned id, float vol, long long& pdelta) {
+  const unsigned l = local_index(x, y, z);
+  const bool is_water = c.mat == WATER;
+  if (vol <= 1e-6f) {
+    erase_part(R, c, l, pdelta);
+    if (is_water) {
+      write_mat(R, c, l, id, 0);
+      return true;
+    }
+    return false;
+  }
+  if (vol >= full_level()) {
+    erase_part(R, c, l, pdelta);
+    if (!is_water) {
+      write_mat(R, c, l, id, WATER);
+      return true;
+    }
+    return false;
+  }
+  if (c.slot == NOSLOT) return false;
+  if (!(c.part > 0.0f)) pdelta += 1;
+  R.avol[(size_t)c.slot * 512u + l] = vol;
+  c.part = vol;
+  if (is_water && vol < HIDE_BELOW) {
+    write_mat(R, c, l, id, 0);
+    return true;
+  }
+  if (!is_water && vol >= SHOW_AT) {
+    write_mat(R, c, l, id, WATER);
+    return true;
+  }
+  return false;
+}
+
+// Warp: lanes with `w` write `vol` into their cell through set_volume. Returns whether any
+// voxel changed.
+__device__ bool warp_set_volume(const Region& R, WS& W, bool w, CD& c, int x, int y, int z, float vol) {
+  bool need = w && set_volume_needs_slot(c, vol);
+  if (__any_sync(FULLMASK, need)) materialize_lanes(R, need, c.gi, c.slot);
+  bool ch = false;
+  if (w) ch = set_volume_lane(R, c, x, y, z, in_dom(R, x, y, z) ? dom_id(R, x, y, z) : 0u, vol, W.pdelta);
+  __syncwarp();
+  return __any_sync(FULLMASK, ch);
+}
+
+// ---------------------------------------------------------------------------- activation
+// An ordered activation list: each entry is a single cell (FluidSim::activate, fluid.rs:292-300)
+// or a wake_around centre (7 cells in the order self,+x,-x,+y,-y,+z,-z; fluid.rs:302-310).
+struct ActList {
+  int x[8], y[8], z[8];
+  unsigned char kind[8];  // 1 = single, 7 = wake_around
+  int n;
+  __device__ __forceinline__ void reset() { n = 0; }
+  __device__ __forceinline__ void single(int a, int b, int c) {
+    x[n] = a; y[n] = b; z[n] = c; kind[n] = 1; ++n;
+  }
+  __device__ __forceinline__ void around(int a, int b, int c) {
+    x[n] = a; y[n] = b; z[n] = c; kind[n] = 7; ++n;
+  }
+};
+
+// Push cells (one per lane, lane order = program order) that are not active yet.
+__device__ __forceinline__ void activate_round(const Region& R, WS& W, bool valid, int x, int y, int z) {
+  const unsigned lane = lane_id();
+  unsigned id = 0;
+  if (valid) {
+    if (y < 0) valid = false;  // fluid.rs:293-295
+    else if (!in_dom(R, x, y, z)) {
+      set_status(R, ST_RANGE, 3);
+      valid = false;
+    } else {
+      id = dom_id(R, x, y, z);
+    }
+  }
+  unsigned peers = __match_any_sync(FULLMASK, valid ? id : (0xFFFFFFFFu - lane));
+  bool first = valid && !(peers & lanemask_lt());
+  bool isnew = false;
+  if (first) isnew = !((R.active[id >> 5] >> (id & 31)) & 1u);
+  unsigned nb = __ballot_sync(FULLMASK, isnew);
+  if (isnew) {
+    unsigned long long pos = W.qtail + (unsigned long long)__popc(nb & lanemask_lt());
+    R.queue[pos & R.qmask] = id;
+    atomicOr(&R.active[id >> 5], 1u << (id & 31));
+  }
+  W.qtail += (unsigned long long)__popc(nb);
+  W.activations += (unsigned long long)__popc(nb);
+  __syncwarp();
+}
+
+__device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
+  if (A.n == 0) return;
+  const unsigned lane = lane_id();
+  int total = 0;
+  for (int g = 0; g < A.n; ++g) total += A.kind[g];
+  for (int base = 0; base < total; base += 32) {
+    int t = base + (int)lane;
+    bool valid = t < total;
+    int x = 0, y = 0, z = 0;
+    if (valid) {
+      int acc = 0;
+      for (int g = 0; g < A.n; ++g) {
+        int k = A.kind[g];
+        if (t < acc + k) {
+          int o = t - acc;
+          x = A.x[g];
+          y = A.y[g];
+          z = A.z[g];
+          if (k == 7) {
+            // self, +x, -x, +y, -y, +z, -z
+            x += (o == 1) - (o == 2);
+            y += (o == 3) - (o == 4);
+            z += (o == 5) - (o == 6);
+          }
+          break;
+        }
+        acc += k;
+      }
+    }
+    activate_round(R, W, valid, x, y, z);
+  }
+  if (W.qtail - W.qhead > R.qmask + 1ull) set_status(R, ST_OOM, 4);
+}
+
+// FluidSim::seed_level (fluid.rs:312-316); warp-uniform call.
+__device__ __forceinline__ void seed_level(const Region& R, WS& W, int x, int y, int z) {
+  if (W.level_round || W.nseeds >= MAX_LEVEL_SEEDS) return;
+  unsigned id = dom_id(R, x, y, z);
+  unsigned ins = 0;
+  if (lane_id() == 0) {
+    unsigned old = atomicOr(&R.seedbits[id >> 5], 1u << (id & 31));
+    ins = !(old & (1u << (id & 31)));
+    if (ins) R.seeds[W.nseeds] = id;
+  }
+  ins = __shfl_sync(FULLMASK, ins, 0);
+  W.nseeds += ins;
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------- pressure BFS
+__device__ __forceinline__ bool vis_insert(unsigned long long* vis, unsigned id, unsigned epoch) {
+  unsigned h = (id * 2654435761u) & (VIS_CAP - 1u);
+  unsigned long long want = ((unsigned long long)epoch << 32) | id;
+  unsigned long long cur = vis[h];
+  while (true) {
+    if ((unsigned)(cur >> 32) != epoch) {
+      unsigned long long old = atomicCAS(&vis[h], cur, want);
+      if (old == cur) return true;
+      cur = old;
+      continue;
+    }
+    if ((unsigned)cur == id) return false;
+    h = (h + 1u) & (VIS_CAP - 1u);
+    cur = vis[h];
+  }
+}
+
+// D of pressure_pull (fluid.rs:512): up, +x, -x, +z, -z.
+__device__ __forceinline__ void dir5(int d, int& dx, int& dy, int& dz) {
+  dx = (d == 1) - (d == 2);
+  dy = (d == 0);
+  dz = (d == 3) - (d == 4);
+}
+
+// FluidSim::pressure_pull (fluid.rs:511-561), warp-cooperative. fp[2..6] = up,+x,-x,+z,-z.
+// Appends the source's activation to A and seeds it. Returns the volume taken.
+__device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int x, int y, int z, float need, const CD* fp) {
+  const unsigned lane = lane_id();
+  W.epoch += 1u;
+  if (W.epoch == 0u) {  // wrapped: clear
+    for (unsigned i = lane; i < VIS_CAP; i += 32) S.vis[i] = 0ull;
+    __syncwarp();
+    W.epoch = 1u;
+  }
+  const float FULL = full_level();
+  if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
+  __syncwarp();
+  bool ok = false;
+  unsigned nid = 0;
+  if (lane < 5) {
+    int dx, dy, dz;
+    dir5((int)lane, dx, dy, dz);
+    int a = x + dx, b = y + dy, c = z + dz;
+    const CD& cd = fp[2 + lane];
+    ok = a >= 0 && c >= 0 && !cd_solid(cd) && cd_volume(cd) >= FULL;
+    if (ok) nid = dom_id(R, a, b, c);
+  }
+  unsigned bm = __ballot_sync(FULLMASK, ok);
+  unsigned qlen = (unsigned)__popc(bm);
+  if (qlen == 0) return 0.0f;
+  if (ok) {
+    S.pq[__popc(bm & lanemask_lt())] = nid;
+    vis_insert(S.vis, nid, W.epoch);
+  }
+  __syncwarp();
+  unsigned side = 0, i = 0;
+  float got = 0.0f;
+  while (i < qlen && i < PRESSURE_SEARCH) {
+    unsigned e = S.pq[i];
+    ++i;
+    int a, b, c;
+    dom_xyz(R, e, a, b, c);
+    int na = a, nb = b, nc = c;
+    if (lane >= 1 && lane <= 5) {
+      int dx, dy, dz;
+      dir5((int)lane - 1, dx, dy, dz);
+      na += dx;
+      nb += dy;
+      nc += dz;
+    }
+    CD cd;
+    if (lane < 6) cd = load_cell(R, S.ring, na, nb, nc);
+    else cd = CD{0.0f, NOSLOT, 0u, 0, true};
+    float here = __shfl_sync(FULLMASK, cd_volume(cd), 0);
+    bool top_l = (lane == 1) && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f);
+    bool top = __shfl_sync(FULLMASK, top_l, 1);
+    if (top && b > y && here > 0.0f) {
+      float take = fminf(need, here);
+      float nv = __fsub_rn(here, take);
+      CD c0 = shfl_cd(cd, 0);
+      W.changed |= warp_set_volume(R, W, lane == 0, c0, a, b, c, nv);
+      A.single(a, b, c);
+      seed_level(R, W, a, b, c);
+      got = take;
+      break;
+    }
+    bool cand = false;
+    if (lane >= 1 && lane <= 5) cand = !(na < 0 || nc < 0 || nb >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f);
+    bool sc = cand && lane >= 2 && nb == y;
+    unsigned sm = __ballot_sync(FULLMASK, sc);
+    if (sc && side + (unsigned)__popc(sm & lanemask_lt()) + 1u > 24u) cand = false;
+    side += (unsigned)__popc(sm);
+    bool isnew = false;
+    unsigned id = 0;
+    if (cand) {
+      id = dom_id(R, na, nb, nc);
+      isnew = vis_insert(S.vis, id, W.epoch);
+    }
+    unsigned nm = __ballot_sync(FULLMASK, isnew);
+    if (isnew) {
+      unsigned pos = qlen + (unsigned)__popc(nm & lanemask_lt());
+      if (pos < PRESS_QCAP) S.pq[pos] = id;
+    }
+    qlen += (unsigned)__popc(nm);
+    __syncwarp();
+  }
+  W.bfs_visits += i;
+  return got;
+}
+
+// --------------------------------------------------------------------------- one cell
+// The body of FluidSim::tick's loop (fluid.rs:584-650) for the cell (x, y, z).
+__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z) {
+  const unsigned lane = lane_id();
+  const float FULL = full_level();
+  // footprint: 0 self, 1 below, 2 up, 3 +x, 4 -x, 5 +z, 6 -z
+  int fx = x, fy = y, fz = z;
+  if (lane == 1) fy -= 1;
+  else if (lane == 2) fy += 1;
+  else if (lane == 3) fx += 1;
+  else if (lane == 4) fx -= 1;
+  else if (lane == 5) fz += 1;
+  else if (lane == 6) fz -= 1;
+  CD mine;
+  if (lane < 7) mine = load_cell(R, S.ring, fx, fy, fz);
+  else mine = CD{0.0f, NOSLOT, 0u, 0, true};
+  CD fp[7];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) fp[j] = shfl_cd(mine, j);
+  const unsigned id = dom_id(R, x, y, z);
+  if (cd_solid(fp[0])) {  // fluid.rs:586-589
+    if (lane == 0) erase_part(R, mine, local_index(x, y, z), W.pdelta);
+    __syncwarp();
+    return;
+  }
+  ActList A;
+  A.reset();
+  float vol = cd_volume(fp[0]);
+  const float v0 = vol;
+  // 0. pressure (fluid.rs:594-601)
+  if (vol < FULL && W.pulls < MAX_PULLS_PER_TICK) {
+    float got = pressure_pull(R, W, S, A, x, y, z, __fsub_rn(1.0f, vol), fp);
+    W.pulls += 1;
+    W.pull_attempts += 1;
+    if (got > 0.0f) {
+      W.pull_success += 1;
+      vol = __fadd_rn(vol, got);
+      A.around(x, y, z);
+    }
+  }
+  if (vol <= 0.0f) {  // fluid.rs:602-604
+    flush_acts(R, W, A);
+    return;
+  }
+  // 1. fall (fluid.rs:606-614)
+  bool w_below = false;
+  float below_new = 0.0f;
+  const bool below_solid = cd_solid(fp[1]);
+  float below_after = cd_volume(fp[1]);
+  if (!below_solid) {
+    float bv = cd_volume(fp[1]);
+    float f = fminf(vol, __fsub_rn(1.0f, bv));
+    if (f > 1e-6f) {
+      below_new = __fadd_rn(bv, f);
+      w_below = true;
+      vol = __fsub_rn(vol, f);
+      A.around(x, y - 1, z);
+      below_after = below_new >= FULL ? 1.0f : below_new;
+    }
+  }
+  // 2. spread (fluid.rs:617-639)
+  bool w_side[4] = {false, false, false, false};
+  float side_new[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (vol > MIN_SPREAD && (below_solid || below_after >= FULL)) {
+    float nv[4];
+    bool open[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      open[i] = !cd_solid(fp[3 + i]);
+      nv[i] = open[i] ? cd_volume(fp[3 + i]) : 0.0f;
+    }
+    const float here = vol;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (!open[i] || nv[i] >= here) continue;
+      float f = __fmul_rn(__fsub_rn(here, nv[i]), 0.2f);
+      if (f < MIN_FLOW || __fsub_rn(here, f) < MIN_SPREAD * 0.5f) continue;
+      side_new[i] = __fadd_rn(nv[i], f);
+      w_side[i] = true;
+      vol = __fsub_rn(vol, f);
+      if (f > SLEEP) {
+        int sx = x + (i == 0) - (i == 1), sz = z + (i == 2) - (i == 3);
+        A.around(sx, y, sz);
+      }
+    }
+  }
+  // 3. evaporate, write back, sleep test (fluid.rs:641-650)
+  if (vol < EVAPORATE) vol = 0.0f;
+  const float dv = fabsf(__fsub_rn(vol, v0));
+  const bool w_self = dv > 1e-7f;
+  // parallel writes into distinct cells: lane 0 self, 1 below, 3..6 sides
+  bool w = false;
+  float wv = 0.0f;
+  if (lane == 0) {
+    w = w_self;
+    wv = vol;
+  } else if (lane == 1) {
+    w = w_below;
+    wv = below_new;
+  } else if (lane >= 3 && lane <= 6) {
+    w = w_side[lane - 3];
+    wv = side_new[lane - 3];
+  }
+  if (__any_sync(FULLMASK, w)) W.changed |= warp_set_volume(R, W, w, mine, fx, fy, fz, wv);
+  if (dv > SLEEP) {
+    A.around(x, y, z);
+    seed_level(R, W, x, y, z);
+  }
+  flush_acts(R, W, A);
+  (void)id;
+}
+
+// ------------------------------------------------------------------------ level fill
+// LayerMarks::test_and_set (fluid.rs:194-200): one bit per cell in 64x64 tiles per layer; the
+// tiles touched during a levelling round are listed so the round's end clears only those.
+__device__ __forceinline__ bool mark_tas(const Region& R, int x, int y, int z) {
+  if (!in_dom(R, x, y, z)) {  // cannot happen for neighbours of addressable cells; never write out of range
+    set_status(R, ST_RANGE, 8);
+    return true;
+  }
+  unsigned xr = (unsigned)(x - R.px0), zr = (unsigned)(z - R.pz0);
+  unsigned tile = ((zr >> 6) * (unsigned)R.PY + (unsigned)y) * (unsigned)R.TX + (xr >> 6);
+  unsigned bit = ((zr & 63u) << 6) | (xr & 63u);
+  unsigned old = atomicOr(&R.marks[(size_t)tile * 128u + (bit >> 5)], 1u << (bit & 31));
+  if (R.mark_tflag[tile] == 0u && atomicExch(&R.mark_tflag[tile], 1u) == 0u) {
+    unsigned k = atomicAdd(&R.ctl->mark_ntiles, 1u);
+    R.mark_list[k] = tile;
+  }
+  return (old >> (bit & 31)) & 1u;
+}
+
+__device__ __forceinline__ void side4(int d, int& dx, int& dz) {  // SIDES (fluid.rs:228)
+  dx = (d == 0) - (d == 1);
+  dz = (d == 2) - (d == 3);
+}
+
+// FluidSim::level_layer (fluid.rs:412-486), warp-cooperative. Cells are gathered in the exact
+// BFS order of the reference and summed in that order in f64.
+__device__ bool level_layer(const Region& R, WS& W, Smem& S, int sx, int sy, int sz) {
+  const unsigned lane = lane_id();
+  const float FULL = full_level();
+  // member (fluid.rs:413-415): !solid && vol > 0 && supported && vol(above) <= 0
+  unsigned was = 0;
+  if (lane == 0) was = mark_tas(R, sx, sy, sz);
+  was = __shfl_sync(FULLMASK, was, 0);
+  if (was) return false;
+  CD m3 = CD{0.0f, NOSLOT, 0u, 0, true};
+  if (lane < 3) m3 = load_cell(R, S.ring, sx, sy + (lane == 1 ? -1 : (lane == 2 ? 1 : 0)), sz);
+  CD cs = shfl_cd(m3, 0), cb = shfl_cd(m3, 1), ca = shfl_cd(m3, 2);
+  bool member = !cd_solid(cs) && cd_volume(cs) > 0.0f && (cd_solid(cb) || cd_volume(cb) >= FULL) && cd_volume(ca) <= 0.0f;
+  if (!member) return false;
+  if (lane == 0) {
+    R.lvl_id[0] = dom_id(R, sx, sy, sz);
+    R.lvl_vol[0] = cd_volume(cs);
+  }
+  __syncwarp();
+  unsigned len = 1, i = 0;
+  double sum = 0.0;
+  float lo = 2.0f, hi = -1.0f;
+  while (i < len) {
+    unsigned cid = R.lvl_id[i];
+    float vol = R.lvl_vol[i];
+    ++i;
+    sum = __dadd_rn(sum, (double)vol);
+    lo = fminf(lo, vol);
+    hi = fmaxf(hi, vol);
+    if (len >= MAX_LEVEL_CELLS) continue;
+    int x, y, z;
+    dom_xyz(R, cid, x, y, z);
+    // lanes 0..11: side d = lane/3, j = lane%3 (0 the neighbour, 1 below it, 2 above it)
+    int d = (int)lane / 3, j = (int)lane % 3;
+    int dx = 0, dz = 0;
+    if (lane < 12) side4(d, dx, dz);
+    int nx = x + dx, nz = z + dz;
+    bool skip = lane >= 12 || (R.ring_w == 0 && (nx < 0 || nz < 0));
+    unsigned tas = 0;
+    if (!skip && j == 0) tas = mark_tas(R, nx, y, nz);
+    CD c = CD{0.0f, NOSLOT, 0u, 0, true};
+    if (!skip) c = load_cell(R, S.ring, nx, y + (j == 1 ? -1 : (j == 2 ? 1 : 0)), nz);
+    // gather the three cells of each side at its j==0 lane
+    float v = cd_volume(c);
+    bool sol = cd_solid(c);
+    float v1 = __shfl_down_sync(FULLMASK, v, 1), v2 = __shfl_down_sync(FULLMASK, v, 2);
+    bool s1 = __shfl_down_sync(FULLMASK, (unsigned)sol, 1) != 0u;
+    bool push = !skip && j == 0 && !tas && !sol && v > 0.0f && (s1 || v1 >= FULL) && v2 <= 0.0f;
+    unsigned pm = __ballot_sync(FULLMASK, push);
+    if (push) {
+      unsigned pos = len + (unsigned)__popc(pm & lanemask_lt());
+      R.lvl_id[pos] = dom_id(R, nx, y, nz);
+      R.lvl_vol[pos] = v;
+    }
+    len += (unsigned)__popc(pm);
+    __syncwarp();
+  }
+  W.llc += len;
+  W.level_cells_total += len;
+  bool changed = false;
+  if (len >= 2 && __fsub_rn(hi, lo) >= SLEEP) {
+    const float avg = __double2float_rn(__ddiv_rn(sum, (double)len));
+    if (avg >= MIN_SPREAD) {  // fluid.rs:449-455
+      for (unsigned b0 = 0; b0 < len; b0 += 32) {
+        unsigned k = b0 + lane;
+        bool wv = false;
+        int x = 0, y = 0, z = 0;
+        CD c = CD{0.0f, NOSLOT, 0u, 0, true};
+        if (k < len) {
+          dom_xyz(R, R.lvl_id[k], x, y, z);
+          c = load_cell(R, S.ring, x, y, z);
+          wv = fabsf(__fsub_rn(cd_volume(c), avg)) > 1e-6f;
+        }
+        changed |= warp_set_volume(R, W, wv, c, x, y, z, avg);
+      }
+    } else {  // drain into the water under the film (fluid.rs:456-481)
+      double left = sum;
+      bool stop = false;
+      for (unsigned b0 = 0; b0 < len && !stop; b0 += 32) {
+        unsigned k = b0 + lane;
+        int x = 0, y = 0, z = 0;
+        CD c = CD{0.0f, NOSLOT, 0u, 0, true};
+        bool ok = false;
+        if (k < len) {
+          dom_xyz(R, R.lvl_id[k], x, y, z);
+          if (y != 0) {
+            c = load_cell(R, S.ring, x, y - 1, z);
+            ok = !cd_solid(c);
+          }
+        }
+        float bel = cd_volume(c);
+        // sequential in cell order: take = min(left, 1 - below)
+        bool wv = false;
+        float nvv = 0.0f;
+        unsigned n_here = min(32u, len - b0);
+        for (unsigned t = 0; t < n_here; ++t) {
+          bool okt = __shfl_sync(FULLMASK, ok, t);
+          float bt = __shfl_sync(FULLMASK, bel, t);
+          if (!okt) continue;
+          float take = __double2float_rn(fmin(left, (double)__fsub_rn(1.0f, bt)));
+          if (take <= 0.0f) continue;
+          if (lane == t) {
+            wv = true;
+            nvv = __fadd_rn(bt, take);
+          }
+          left = __dsub_rn(left, (double)take);
+          if (left <= 1e-6) {
+            stop = true;
+            break;
+          }
+        }
+        changed |= warp_set_volume(R, W, wv, c, x, y - 1, z, nvv);
+        // activations in cell order (fluid.rs:472)
+        unsigned am = __ballot_sync(FULLMASK, wv);
+        for (unsigned m = am; m; m &= m - 1) {
+          int l = __ffs(m) - 1;
+          int ax = __shfl_sync(FULLMASK, x, l), ay = __shfl_sync(FULLMASK, y, l), az = __shfl_sync(FULLMASK, z, l);
+          activate_round(R, W, lane == 0, ax, ay - 1, az);
+        }
+      }
+      const float rest = __double2float_rn(__ddiv_rn(left, (double)len));
+      const float rv = rest < EVAPORATE ? 0.0f : rest;
+      for (unsigned b0 = 0; b0 < len; b0 += 32) {
+        unsigned k = b0 + lane;
+        int x = 0, y = 0, z = 0;
+        CD c = CD{0.0f, NOSLOT, 0u, 0, true};
+        bool wv = k < len;
+        if (wv) {
+          dom_xyz(R, R.lvl_id[k], x, y, z);
+          c = load_cell(R, S.ring, x, y, z);
+        }
+        changed |= warp_set_volume(R, W, wv, c, x, y, z, rv);
+      }
+    }
+  }
+  return changed;
+}
+
+// FluidSim::level_surfaces (fluid.rs:489-507). Returns true when the round ended (marks to clear).
+__device__ bool level_surfaces(const Region& R, WS& W, Smem& S) {
+  const unsigned lane = lane_id();
+  W.llc = 0;
+  while (W.llc < LEVEL_BUDGET) {
+    if (W.nseeds == 0) break;
+    W.nseeds -= 1;
+    unsigned k = R.seeds[W.nseeds];
+    if (lane == 0) atomicAnd(&R.seedbits[k >> 5], ~(1u << (k & 31)));
+    __syncwarp();
+    int x, y, z;
+    dom_xyz(R, k, x, y, z);
+    // walk up to the top water cell (fluid.rs:496-499), 32 cells per round
+    while (true) {
+      int yy = y + 1 + (int)lane;
+      bool cond = false;
+      if (yy < R.ny) {
+        CD c = load_cell(R, S.ring, x, yy, z);
+        cond = !cd_solid(c) && cd_volume(c) > 0.0f;
+      }
+      unsigned fail = __ballot_sync(FULLMASK, !cond);
+      int steps = fail ? __ffs(fail) - 1 : 32;
+      y += steps;
+      if (steps < 32) break;
+    }
+    W.changed |= level_layer(R, W, S, x, y, z);
+  }
+  W.level_round = W.nseeds != 0;
+  return !W.level_round;
+}
+
+}  // namespace vfe
