@@ -101,6 +101,9 @@ int sync_ctl(vf_fluid* h) {
   return VF_OK;
 }
 
+// Offsets into the scratch buffer are kept 16-byte aligned (8-byte device atomics live there).
+size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
 uint64_t next_pow2(uint64_t v) {
   uint64_t p = 1;
   while (p < v) p <<= 1;
@@ -314,10 +317,10 @@ int vf_fluid_wake(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, i
 static int run_edit(vf_fluid* h, int kind, const int32_t* xyz, uint64_t n, int m, float amount, uint64_t* out_count, size_t ints_per) {
   int rc = check(h);
   if (rc) return rc;
-  size_t bytes = std::max<size_t>(n * ints_per * 4, 16) + 64;
-  if ((rc = ensure_scratch(h, bytes))) return rc;
+  const size_t data = align16(n * ints_per * 4);
+  if ((rc = ensure_scratch(h, data + 64))) return rc;
   if (n) CK(cudaMemcpyAsync(h->scratch, xyz, n * ints_per * 4, cudaMemcpyHostToDevice, h->stream));
-  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + bytes - 64);
+  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + data);
   k_edit<<<1, 32, 0, h->stream>>>(h->R, kind, (const int*)h->scratch, n, m, amount, out_count ? dcount : nullptr);
   CK(cudaGetLastError());
   if (out_count) {
@@ -472,12 +475,12 @@ int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
   unsigned nslots = std::min(h->hctl->atlas_used, h->R.atlas_cap);
-  size_t need = (size_t)nslots * 4 + 64 + cap * 16;
-  if ((rc = ensure_scratch(h, need))) return rc;
+  const size_t o_count = align16((size_t)nslots * 4), o_xyz = o_count + 64, o_vol = o_xyz + align16(cap * 12);
+  if ((rc = ensure_scratch(h, o_vol + align16(cap * 4) + 16))) return rc;
   int* slot_brick = (int*)h->scratch;
-  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + (size_t)nslots * 4);
-  int* dxyz = (int*)((char*)h->scratch + (size_t)nslots * 4 + 64);
-  float* dvol = (float*)((char*)dxyz + cap * 12);
+  unsigned long long* dcount = (unsigned long long*)((char*)h->scratch + o_count);
+  int* dxyz = (int*)((char*)h->scratch + o_xyz);
+  float* dvol = (float*)((char*)h->scratch + o_vol);
   CK(cudaMemsetAsync(slot_brick, 0xFF, (size_t)nslots * 4 + 8, h->stream));
   CK(cudaMemsetAsync(dcount, 0, 8, h->stream));
   uint64_t nb = (uint64_t)h->R.bx * h->R.by * h->R.bz;
