@@ -111,6 +111,12 @@ int vf_fluid_set_partial(vf_fluid* h, int32_t x, int32_t y, int32_t z, float v);
 /* FluidSim::tick (src/fluid.rs:564-657), n_ticks times back to back on the device.
  * *changed (optional) = 1 if any voxel changed. */
 int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed);
+/* The same ticks, enqueued on the handle's stream without waiting (capturable in a CUDA graph);
+ * vf_fluid_sync waits and reports the device status. */
+int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks);
+int vf_fluid_sync(vf_fluid* h);
+/* The cudaStream_t the handle runs on. */
+void* vf_fluid_stream(vf_fluid* h);
 /* FluidSim::update (src/fluid.rs:662-676): fixed 20 Hz, at most 3 ticks per call. */
 int vf_fluid_update(vf_fluid* h, float dt, int32_t* changed);
 
@@ -141,6 +147,12 @@ int vf_fluid_export_box(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t
 /* Order-independent digests, computed on the device, of the voxel+partial state and of the
  * FIFO and seed list (same definitions as the test oracle's). */
 int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* seeds);
+
+/* Cycle counters per tick phase, summed over all ticks (SM clock of the region's CTA): 0 drain,
+ * 1 sort, 2 sweep, 3 sweep waiting on prefetch, 4 pressure pulls, 5 activation logging, 6 voxel
+ * writes, 7 seed commit, 8 levelling, 9 FIFO commit, 10 change commit, 11 mark clearing,
+ * 15 between ticks. */
+int vf_fluid_profile(vf_fluid* h, uint64_t* out16);
 
 /* ---- batched regions: pattern (2) of the engine. Every handle is an independent FluidSim
  * (its own world, FIFO, caps); one launch steps all of them n_ticks times, one CTA per region.

@@ -134,6 +134,9 @@ def lib():
         "vf_fluid_set_partial": (C.c_int, [P, I32, I32, I32, C.c_float]),
         "vf_fluid_tick": (C.c_int, [P, I32, C.POINTER(C.c_int32)]),
         "vf_fluid_update": (C.c_int, [P, C.c_float, C.POINTER(C.c_int32)]),
+        "vf_fluid_tick_async": (C.c_int, [P, I32]),
+        "vf_fluid_sync": (C.c_int, [P]),
+        "vf_fluid_stream": (C.c_void_p, [P]),
         "vf_fluid_download_changes": (C.c_int, [P, C.POINTER(Voxel), U64, C.POINTER(C.c_uint64)]),
         "vf_fluid_volume": (C.c_int, [P, I32, I32, I32, C.POINTER(C.c_float)]),
         "vf_fluid_idle": (C.c_int, [P, C.POINTER(C.c_int32)]),
@@ -148,6 +151,7 @@ def lib():
         "vf_fluid_export_box": (C.c_int, [P, I32, I32, I32, I32, I32, I32, C.POINTER(C.c_uint8), C.POINTER(C.c_float)]),
         "vf_fluid_digest": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vf_fluid_batch_tick": (C.c_int, [C.POINTER(P), I32, I32]),
+        "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -358,6 +362,17 @@ class FluidSim:
         self._check(lib().vf_fluid_tick(self.h, n, C.byref(ch)), "tick")
         return bool(ch.value)
 
+    def tick_async(self, n: int = 1):
+        """Enqueue n ticks on the handle's stream without waiting."""
+        self._check(lib().vf_fluid_tick_async(self.h, n), "tick_async")
+
+    def sync(self):
+        self._check(lib().vf_fluid_sync(self.h), "sync")
+
+    @property
+    def stream(self) -> int:
+        return lib().vf_fluid_stream(self.h) or 0
+
     def update(self, dt: float) -> bool:
         ch = C.c_int32()
         self._check(lib().vf_fluid_update(self.h, dt, C.byref(ch)), "update")
@@ -405,6 +420,15 @@ class FluidSim:
 
     def last_tick_cells(self) -> int:
         return self.stats().last_tick_cells
+
+    PROFILE_PHASES = ("drain", "sort", "sweep", "sweep_wait", "pulls", "act_log", "writes", "seed_commit", "level", "fifo_commit",
+                      "chg_commit", "mark_clear", "sweep_top", "sweep_cell", "sweep_tail", "between")
+
+    def profile(self) -> dict:
+        """SM cycles per tick phase, summed over all ticks so far."""
+        a = (C.c_uint64 * 16)()
+        self._check(lib().vf_fluid_profile(self.h, a), "profile")
+        return {k: int(v) for k, v in zip(self.PROFILE_PHASES, a) if k != "-"}
 
     def shift(self, dx, dz):
         self._check(lib().vf_fluid_shift(self.h, dx, dz), "shift")

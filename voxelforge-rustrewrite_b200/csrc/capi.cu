@@ -21,6 +21,7 @@ struct vf_fluid {
   Region R{};
   Region* dR = nullptr;
   Ctl* hctl = nullptr;  // pinned mirror
+  unsigned* hzero = nullptr;  // pinned control word copied in by every tick
   bool uploaded = false;
   std::string err;
   std::vector<void*> dev_allocs;
@@ -152,6 +153,11 @@ int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
     return VF_ERR_OOM;
   }
   std::memset(h->hctl, 0, sizeof(Ctl));
+  if (cudaMallocHost(&h->hzero, 16) != cudaSuccess) {
+    cudaFreeHost(h->hctl);
+    delete h;
+    return VF_ERR_OOM;
+  }
   // the tick kernel's image must load (sm_100a only): probe its attributes
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, k_tick) != cudaSuccess) {
@@ -170,6 +176,7 @@ void vf_fluid_destroy(vf_fluid* h) {
   cudaSetDevice(h->device);
   free_world(h);
   if (h->hctl) cudaFreeHost(h->hctl);
+  if (h->hzero) cudaFreeHost(h->hzero);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -214,7 +221,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   }
   R.PY = ny + P;
   uint64_t ncells = (uint64_t)R.PX * R.PY * R.PZ;
-  if (ncells >= 0xFFFFFFF0ull) return fail(h, VF_ERR_RANGE, "domain too large for 32-bit cell ids");
+  if (ncells >= 0x7FFFFFF0ull) return fail(h, VF_ERR_RANGE, "domain too large for 31-bit cell ids");
   R.ncells = (unsigned)ncells;
   R.TX = (R.PX + 63) / 64;
   R.TZ = (R.PZ + 63) / 64;
@@ -260,6 +267,15 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.marks, tiles * 128))) return rc;
   if ((rc = dalloc(h, &R.mark_list, tiles))) return rc;
   if ((rc = dalloc(h, &R.mark_tflag, tiles))) return rc;
+  // per-tick event logs: <= 50 activations and 7 writes per swept cell, plus levelling's
+  R.ev_act_cap = 1u << 22;
+  R.ev_seed_cap = 1u << 18;
+  R.ev_chg_cap = 1u << 21;
+  if ((rc = dalloc(h, &R.ev_act, R.ev_act_cap, false))) return rc;
+  if ((rc = dalloc(h, &R.ev_seed, R.ev_seed_cap, false))) return rc;
+  if ((rc = dalloc(h, &R.ev_chg, R.ev_chg_cap, false))) return rc;
+  if ((rc = dalloc(h, &R.stamp, ncells, false))) return rc;
+  CK(cudaMemsetAsync(R.stamp, 0xFF, ncells * 4, h->stream));
   R.chg_cap = 1u << 22;
   if ((rc = dalloc(h, &R.chg, R.chg_cap, false))) return rc;
   uint64_t qcap = next_pow2(std::max<uint64_t>({h->want_queue, std::min<uint64_t>(ncells, 1ull << 22), 1ull << 16}));
@@ -356,19 +372,35 @@ int vf_fluid_set_partial(vf_fluid* h, int32_t x, int32_t y, int32_t z, float v) 
   return run_edit(h, ED_SET_PARTIAL, p, 1, 0, v, nullptr, 3);
 }
 
-int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed) {
+int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks) {
   int rc = check(h);
   if (rc) return rc;
   if (n_ticks < 0) return VF_ERR_INVALID;
-  CK(cudaMemsetAsync(&h->R.ctl->changed, 0, sizeof(unsigned), h->stream));
+  // the step's control input (reset of the "changed" flag) goes host -> device from pinned memory
+  h->hzero[0] = 0u;
+  CK(cudaMemcpyAsync(&h->R.ctl->changed, h->hzero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
   if (n_ticks > 0) {
     k_tick<<<1, TICK_THREADS, h->smem_bytes, h->stream>>>(h->dR, 1, n_ticks);
     CK(cudaGetLastError());
   }
+  return VF_OK;
+}
+
+int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed) {
+  int rc = vf_fluid_tick_async(h, n_ticks);
+  if (rc) return rc;
   rc = sync_ctl(h);
   if (changed) *changed = h->hctl->changed ? 1 : 0;
   return rc;
 }
+
+int vf_fluid_sync(vf_fluid* h) {
+  int rc = check(h);
+  if (rc) return rc;
+  return sync_ctl(h);
+}
+
+void* vf_fluid_stream(vf_fluid* h) { return h ? (void*)h->stream : nullptr; }
 
 int vf_fluid_idle(vf_fluid* h, int32_t* out) {
   int rc = check(h);
@@ -635,6 +667,14 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
   if (state) *state = out[0];
   if (queue) *queue = out[1];
   if (seeds) *seeds = out[2];
+  return VF_OK;
+}
+
+int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (out16) std::memcpy(out16, h->hctl->prof, sizeof(h->hctl->prof));
   return VF_OK;
 }
 

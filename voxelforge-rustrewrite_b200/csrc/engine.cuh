@@ -52,7 +52,12 @@ struct Ctl {
   int status;
   unsigned int err_info;
   unsigned int pad[2];
+  // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
+  // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
+  // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear
+  unsigned long long prof[16];
 };
+constexpr int NPROF = 16;
 
 struct Region {
   // ---- geometry (voxel dims, brick dims, ring width; padded scheduler domain)
@@ -82,6 +87,12 @@ struct Region {
   unsigned int* seeds;       // MAX_LEVEL_SEEDS
   unsigned int* lvl_id;      // MAX_LEVEL_CELLS + 8
   float* lvl_vol;
+  // ---- per-tick event logs (program order), committed in parallel at the tick's end
+  unsigned int* ev_act;      // activation events: cell ids
+  unsigned int* ev_seed;     // level-seed events
+  unsigned int* ev_chg;      // voxel-material writes
+  unsigned int ev_act_cap, ev_seed_cap, ev_chg_cap;
+  unsigned int* stamp;       // ncells: first event index per cell during a commit (0xFFFFFFFF idle)
   Ctl* ctl;
 };
 

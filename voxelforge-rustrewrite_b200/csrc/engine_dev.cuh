@@ -81,7 +81,55 @@ struct WS {
   unsigned epoch;          // press-BFS visited epoch
   bool level_round;
   bool changed;
+  // Inside a tick the scheduler side effects are logged in program order and committed in
+  // parallel at the tick's end (deferred); host edits apply them at once.
+  bool deferred;
+  unsigned nact, nseed, nchg;  // event-log cursors (deferred mode)
+  // store-forwarding table of the prefetching sweep (null outside it)
+  unsigned* fwd_key;           // [2][FWD_CAP]
+  unsigned* fwd_val;           // [2][FWD_CAP] material
+  float* fwd_part;             // [2][FWD_CAP]
+  int ft;                      // current table (epoch parity)
+  unsigned long long t_wait, t_pull, t_act, t_write, t_top, t_pc, t_tail;  // cycle counters (profiling)
 };
+
+constexpr int FWD_CAP = 1024;  // forwarding entries per epoch table
+constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned fwd_hash(unsigned id) { return (id * 2654435761u) >> 22; }  // 10 bits
+
+// Record (id -> mat, part) as the latest value this sweep wrote (lane-local call).
+__device__ __forceinline__ void fwd_insert(WS& W, unsigned id, unsigned char mat, float part) {
+  unsigned* keys = W.fwd_key + W.ft * FWD_CAP;
+  unsigned h = fwd_hash(id);
+  for (int k = 0; k < FWD_CAP; ++k) {
+    unsigned cur = keys[h];
+    if (cur == id) break;
+    if (cur == EMPTY_ID) {
+      unsigned old = atomicCAS(&keys[h], EMPTY_ID, id);
+      if (old == EMPTY_ID || old == id) break;
+    }
+    h = (h + 1) & (FWD_CAP - 1);
+  }
+  W.fwd_val[W.ft * FWD_CAP + h] = mat;
+  W.fwd_part[W.ft * FWD_CAP + h] = part;
+}
+
+__device__ __forceinline__ bool fwd_lookup_t(const WS& W, int t, unsigned id, unsigned char& mat, float& part) {
+  const unsigned* keys = W.fwd_key + t * FWD_CAP;
+  unsigned h = fwd_hash(id);
+  for (int k = 0; k < FWD_CAP; ++k) {
+    unsigned cur = keys[h];
+    if (cur == id) {
+      mat = (unsigned char)W.fwd_val[t * FWD_CAP + h];
+      part = W.fwd_part[t * FWD_CAP + h];
+      return true;
+    }
+    if (cur == EMPTY_ID) return false;
+    h = (h + 1) & (FWD_CAP - 1);
+  }
+  return false;
+}
 
 struct Smem {
   unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
@@ -136,7 +184,10 @@ __device__ void materialize_lanes(const Region& R, bool need, unsigned gi, unsig
     }
   }
   __syncwarp();
-  if (leader && s != NOSLOT && g < 256u) R.grid[gi] = 256u + s;
+  // publish the slot after its fill (release): prefetching warps read the grid word first and
+  // then the atlas, with a fence in between
+  __threadfence_block();
+  if (leader && s != NOSLOT && g < 256u) *(volatile unsigned*)(R.grid + gi) = 256u + s;
   int src = need ? (__ffs(peers) - 1) : (int)lane;
   unsigned s2 = __shfl_sync(FULLMASK, s, src);
   if (need) slot = s2;
@@ -153,11 +204,13 @@ __device__ __forceinline__ void record_change(const Region& R, unsigned id) {
   }
 }
 
-__device__ __forceinline__ void write_mat(const Region& R, CD& c, unsigned l, unsigned id, unsigned char m) {
+// Material write; the change is recorded at once (host edits) or logged by the caller (ticks,
+// where `deferred` is set and the caller appends the cell to the change log).
+__device__ __forceinline__ void write_mat(const Region& R, CD& c, unsigned l, unsigned id, unsigned char m, bool deferred = false) {
   if (c.slot == NOSLOT) return;  // materialisation failed (status already set)
   R.amat[(size_t)c.slot * 512u + l] = m;
   c.mat = m;
-  record_change(R, id);
+  if (!deferred) record_change(R, id);
 }
 
 __device__ __forceinline__ void erase_part(const Region& R, CD& c, unsigned l, long long& pdelta) {
@@ -179,13 +232,13 @@ __device__ __forceinline__ bool set_volume_needs_slot(const CD& c, float vol) {
 
 // FluidSim::set_volume (fluid.rs:327-355) on one lane's cell; c.slot must be valid when
 // set_volume_needs_slot said so. Returns "the voxel changed".
-__device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, unsigned id, float vol, long long& pdelta) {
+__device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, unsigned id, float vol, long long& pdelta, bool deferred = false) {
   const unsigned l = local_index(x, y, z);
   const bool is_water = c.mat == WATER;
   if (vol <= 1e-6f) {
     erase_part(R, c, l, pdelta);
     if (is_water) {
-      write_mat(R, c, l, id, 0);
+      write_mat(R, c, l, id, 0, deferred);
       return true;
     }
     return false;
@@ -193,7 +246,7 @@ __device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, uns
   if (vol >= full_level()) {
     erase_part(R, c, l, pdelta);
     if (!is_water) {
-      write_mat(R, c, l, id, WATER);
+      write_mat(R, c, l, id, WATER, deferred);
       return true;
     }
     return false;
@@ -203,40 +256,72 @@ __device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, uns
   R.avol[(size_t)c.slot * 512u + l] = vol;
   c.part = vol;
   if (is_water && vol < HIDE_BELOW) {
-    write_mat(R, c, l, id, 0);
+    write_mat(R, c, l, id, 0, deferred);
     return true;
   }
   if (!is_water && vol >= SHOW_AT) {
-    write_mat(R, c, l, id, WATER);
+    write_mat(R, c, l, id, WATER, deferred);
     return true;
   }
   return false;
 }
 
+// Append per-lane events (lane order) to a log; returns the new cursor.
+__device__ __forceinline__ unsigned log_append(const Region& R, unsigned* log, unsigned cap, unsigned cur, bool v, unsigned id, unsigned site) {
+  unsigned b = __ballot_sync(FULLMASK, v);
+  if (v) {
+    unsigned pos = cur + (unsigned)__popc(b & lanemask_lt());
+    if (pos < cap) log[pos] = id;
+    else set_status(R, ST_OOM, site);
+  }
+  return cur + (unsigned)__popc(b);
+}
+
 // Warp: lanes with `w` write `vol` into their cell through set_volume. Returns whether any
 // voxel changed.
 __device__ bool warp_set_volume(const Region& R, WS& W, bool w, CD& c, int x, int y, int z, float vol) {
+  const long long t0 = clock64();
   bool need = w && set_volume_needs_slot(c, vol);
   if (__any_sync(FULLMASK, need)) materialize_lanes(R, need, c.gi, c.slot);
   bool ch = false;
-  if (w) ch = set_volume_lane(R, c, x, y, z, in_dom(R, x, y, z) ? dom_id(R, x, y, z) : 0u, vol, W.pdelta);
+  const unsigned id = (w && in_dom(R, x, y, z)) ? dom_id(R, x, y, z) : 0u;
+  if (w) {
+    ch = set_volume_lane(R, c, x, y, z, id, vol, W.pdelta, W.deferred);
+    if (W.fwd_key) fwd_insert(W, id, c.mat, c.part);
+  }
+  if (W.deferred) W.nchg = log_append(R, R.ev_chg, R.ev_chg_cap, W.nchg, ch, id, 9);
   __syncwarp();
+  W.t_write += clock64() - t0;
   return __any_sync(FULLMASK, ch);
 }
 
 // ---------------------------------------------------------------------------- activation
 // An ordered activation list: each entry is a single cell (FluidSim::activate, fluid.rs:292-300)
 // or a wake_around centre (7 cells in the order self,+x,-x,+y,-y,+z,-z; fluid.rs:302-310).
+// One cell's activations occupy fixed slots in program order (fluid.rs:584-650): 0 the pull
+// source (single), 1 wake_around(self) after a pull, 2 wake_around(below) after a fall, 3..6
+// wake_around(side) for +x,-x,+z,-z, 7 wake_around(self) at the end. Kept in registers.
 struct ActList {
-  int x[8], y[8], z[8];
-  unsigned char kind[8];  // 1 = single, 7 = wake_around
-  int n;
-  __device__ __forceinline__ void reset() { n = 0; }
-  __device__ __forceinline__ void single(int a, int b, int c) {
-    x[n] = a; y[n] = b; z[n] = c; kind[n] = 1; ++n;
+  int cx, cy, cz;  // the cell
+  int sx, sy, sz;  // the pull source
+  unsigned mask;
+  __device__ __forceinline__ void reset(int x, int y, int z) {
+    cx = x; cy = y; cz = z; mask = 0;
   }
-  __device__ __forceinline__ void around(int a, int b, int c) {
-    x[n] = a; y[n] = b; z[n] = c; kind[n] = 7; ++n;
+  __device__ __forceinline__ void source(int a, int b, int c) {
+    sx = a; sy = b; sz = c; mask |= 1u;
+  }
+  __device__ __forceinline__ void slot(int g) { mask |= 1u << g; }
+  // slot g's centre and kind (1 or 7)
+  __device__ __forceinline__ int get(int g, int& x, int& y, int& z) const {
+    if (g == 0) {
+      x = sx; y = sy; z = sz;
+      return 1;
+    }
+    x = cx + (g == 3) - (g == 4);
+    y = cy - (g == 2);
+    z = cz + (g == 5) - (g == 6);
+    return 7;
   }
 };
 
@@ -255,6 +340,11 @@ __device__ __forceinline__ void activate_round(const Region& R, WS& W, bool vali
   }
   unsigned peers = __match_any_sync(FULLMASK, valid ? id : (0xFFFFFFFFu - lane));
   bool first = valid && !(peers & lanemask_lt());
+  if (W.deferred) {  // inside a tick: log in program order, the tick's end commits
+    W.nact = log_append(R, R.ev_act, R.ev_act_cap, W.nact, first, id, 10);
+    __syncwarp();
+    return;
+  }
   bool isnew = false;
   if (first) isnew = !((R.active[id >> 5] >> (id & 31)) & 1u);
   unsigned nb = __ballot_sync(FULLMASK, isnew);
@@ -268,24 +358,46 @@ __device__ __forceinline__ void activate_round(const Region& R, WS& W, bool vali
   __syncwarp();
 }
 
+// Activation-log word: the cell id, bit 31 set for a wake_around centre (7 cells).
+constexpr unsigned ACT_AROUND = 0x80000000u;
+
 __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
-  if (A.n == 0) return;
+  if (A.mask == 0) return;
+  const long long t0 = clock64();
   const unsigned lane = lane_id();
+  if (W.deferred) {  // one log word per call, in program order (expanded by the commit)
+    bool v = lane < 8 && ((A.mask >> lane) & 1u);
+    unsigned word = 0;
+    if (v) {
+      int x, y, z;
+      int kind = A.get((int)lane, x, y, z);
+      if (!in_dom(R, x, y, z) || y < 0) {
+        set_status(R, ST_RANGE, 13);
+        v = false;
+      } else {
+        word = dom_id(R, x, y, z) | (kind == 7 ? ACT_AROUND : 0u);
+      }
+    }
+    W.nact = log_append(R, R.ev_act, R.ev_act_cap, W.nact, v, word, 10);
+    __syncwarp();
+    W.t_act += clock64() - t0;
+    return;
+  }
+  // immediate mode: expand the slots into single cells, 32 per round
   int total = 0;
-  for (int g = 0; g < A.n; ++g) total += A.kind[g];
+  for (int g = 0; g < 8; ++g)
+    if ((A.mask >> g) & 1u) total += g == 0 ? 1 : 7;
   for (int base = 0; base < total; base += 32) {
     int t = base + (int)lane;
     bool valid = t < total;
     int x = 0, y = 0, z = 0;
     if (valid) {
       int acc = 0;
-      for (int g = 0; g < A.n; ++g) {
-        int k = A.kind[g];
+      for (int g = 0; g < 8; ++g) {
+        if (!((A.mask >> g) & 1u)) continue;
+        int k = A.get(g, x, y, z);
         if (t < acc + k) {
           int o = t - acc;
-          x = A.x[g];
-          y = A.y[g];
-          z = A.z[g];
           if (k == 7) {
             // self, +x, -x, +y, -y, +z, -z
             x += (o == 1) - (o == 2);
@@ -300,12 +412,19 @@ __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
     activate_round(R, W, valid, x, y, z);
   }
   if (W.qtail - W.qhead > R.qmask + 1ull) set_status(R, ST_OOM, 4);
+  W.t_act += clock64() - t0;
 }
 
 // FluidSim::seed_level (fluid.rs:312-316); warp-uniform call.
 __device__ __forceinline__ void seed_level(const Region& R, WS& W, int x, int y, int z) {
-  if (W.level_round || W.nseeds >= MAX_LEVEL_SEEDS) return;
+  if (W.level_round) return;
   unsigned id = dom_id(R, x, y, z);
+  if (W.deferred) {  // the cap and the set membership are applied in order by the commit
+    W.nseed = log_append(R, R.ev_seed, R.ev_seed_cap, W.nseed, lane_id() == 0, id, 11);
+    __syncwarp();
+    return;
+  }
+  if (W.nseeds >= MAX_LEVEL_SEEDS) return;
   unsigned ins = 0;
   if (lane_id() == 0) {
     unsigned old = atomicOr(&R.seedbits[id >> 5], 1u << (id & 31));
@@ -346,28 +465,30 @@ __device__ __forceinline__ void dir5(int d, int& dx, int& dy, int& dz) {
 // Appends the source's activation to A and seeds it. Returns the volume taken.
 __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int x, int y, int z, float need, const CD* fp) {
   const unsigned lane = lane_id();
-  W.epoch += 1u;
-  if (W.epoch == 0u) {  // wrapped: clear
-    for (unsigned i = lane; i < VIS_CAP; i += 32) S.vis[i] = 0ull;
-    __syncwarp();
-    W.epoch = 1u;
-  }
   const float FULL = full_level();
-  if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
-  __syncwarp();
+  // start cells: full up/side neighbours (fluid.rs:518-525); none -> the BFS examines nothing
   bool ok = false;
   unsigned nid = 0;
   if (lane < 5) {
     int dx, dy, dz;
     dir5((int)lane, dx, dy, dz);
     int a = x + dx, b = y + dy, c = z + dz;
-    const CD& cd = fp[2 + lane];
+    // constant-index selects keep fp in registers (a lane-dependent index would spill it)
+    const CD cd = lane == 0 ? fp[2] : lane == 1 ? fp[3] : lane == 2 ? fp[4] : lane == 3 ? fp[5] : fp[6];
     ok = a >= 0 && c >= 0 && !cd_solid(cd) && cd_volume(cd) >= FULL;
     if (ok) nid = dom_id(R, a, b, c);
   }
   unsigned bm = __ballot_sync(FULLMASK, ok);
   unsigned qlen = (unsigned)__popc(bm);
   if (qlen == 0) return 0.0f;
+  W.epoch += 1u;
+  if (W.epoch == 0u) {  // wrapped: clear
+    for (unsigned i = lane; i < VIS_CAP; i += 32) S.vis[i] = 0ull;
+    __syncwarp();
+    W.epoch = 1u;
+  }
+  if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
+  __syncwarp();
   if (ok) {
     S.pq[__popc(bm & lanemask_lt())] = nid;
     vis_insert(S.vis, nid, W.epoch);
@@ -399,7 +520,7 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
       float nv = __fsub_rn(here, take);
       CD c0 = shfl_cd(cd, 0);
       W.changed |= warp_set_volume(R, W, lane == 0, c0, a, b, c, nv);
-      A.single(a, b, c);
+      A.source(a, b, c);
       seed_level(R, W, a, b, c);
       got = take;
       break;
@@ -430,7 +551,9 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
 
 // --------------------------------------------------------------------------- one cell
 // The body of FluidSim::tick's loop (fluid.rs:584-650) for the cell (x, y, z).
-__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z) {
+// `pre` (optional): the footprint as prefetched and store-forwarded by the sweep, in shared
+// memory (7 cells); without it the warp loads the footprint itself.
+__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z, const CD* pre = nullptr) {
   const unsigned lane = lane_id();
   const float FULL = full_level();
   // footprint: 0 self, 1 below, 2 up, 3 +x, 4 -x, 5 +z, 6 -z
@@ -442,11 +565,17 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   else if (lane == 5) fz += 1;
   else if (lane == 6) fz -= 1;
   CD mine;
-  if (lane < 7) mine = load_cell(R, S.ring, fx, fy, fz);
-  else mine = CD{0.0f, NOSLOT, 0u, 0, true};
   CD fp[7];
+  if (pre) {
 #pragma unroll
-  for (int j = 0; j < 7; ++j) fp[j] = shfl_cd(mine, j);
+    for (int j = 0; j < 7; ++j) fp[j] = pre[j];
+    mine = lane < 7 ? pre[lane] : CD{0.0f, NOSLOT, 0u, 0, true};
+  } else {
+    if (lane < 7) mine = load_cell(R, S.ring, fx, fy, fz);
+    else mine = CD{0.0f, NOSLOT, 0u, 0, true};
+#pragma unroll
+    for (int j = 0; j < 7; ++j) fp[j] = shfl_cd(mine, j);
+  }
   const unsigned id = dom_id(R, x, y, z);
   if (cd_solid(fp[0])) {  // fluid.rs:586-589
     if (lane == 0) erase_part(R, mine, local_index(x, y, z), W.pdelta);
@@ -454,18 +583,20 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
     return;
   }
   ActList A;
-  A.reset();
+  A.reset(x, y, z);
   float vol = cd_volume(fp[0]);
   const float v0 = vol;
   // 0. pressure (fluid.rs:594-601)
   if (vol < FULL && W.pulls < MAX_PULLS_PER_TICK) {
+    const long long tp = clock64();
     float got = pressure_pull(R, W, S, A, x, y, z, __fsub_rn(1.0f, vol), fp);
+    W.t_pull += clock64() - tp;
     W.pulls += 1;
     W.pull_attempts += 1;
     if (got > 0.0f) {
       W.pull_success += 1;
       vol = __fadd_rn(vol, got);
-      A.around(x, y, z);
+      A.slot(1);
     }
   }
   if (vol <= 0.0f) {  // fluid.rs:602-604
@@ -484,7 +615,7 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
       below_new = __fadd_rn(bv, f);
       w_below = true;
       vol = __fsub_rn(vol, f);
-      A.around(x, y - 1, z);
+      A.slot(2);
       below_after = below_new >= FULL ? 1.0f : below_new;
     }
   }
@@ -509,8 +640,8 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
       w_side[i] = true;
       vol = __fsub_rn(vol, f);
       if (f > SLEEP) {
-        int sx = x + (i == 0) - (i == 1), sz = z + (i == 2) - (i == 3);
-        A.around(sx, y, sz);
+        (void)0;
+        A.slot(3 + i);
       }
     }
   }
@@ -527,13 +658,22 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   } else if (lane == 1) {
     w = w_below;
     wv = below_new;
-  } else if (lane >= 3 && lane <= 6) {
-    w = w_side[lane - 3];
-    wv = side_new[lane - 3];
+  } else if (lane == 3) {
+    w = w_side[0];
+    wv = side_new[0];
+  } else if (lane == 4) {
+    w = w_side[1];
+    wv = side_new[1];
+  } else if (lane == 5) {
+    w = w_side[2];
+    wv = side_new[2];
+  } else if (lane == 6) {
+    w = w_side[3];
+    wv = side_new[3];
   }
   if (__any_sync(FULLMASK, w)) W.changed |= warp_set_volume(R, W, w, mine, fx, fy, fz, wv);
   if (dv > SLEEP) {
-    A.around(x, y, z);
+    A.slot(7);
     seed_level(R, W, x, y, z);
   }
   flush_acts(R, W, A);

@@ -6,7 +6,7 @@
 
 namespace vfe {
 
-constexpr int TICK_THREADS = 512;
+constexpr int TICK_THREADS = 256;
 constexpr int TICK_WARPS = TICK_THREADS / 32;
 
 // ---------------------------------------------------------------- CTA radix sort (LSD, 8 bit)
@@ -118,12 +118,25 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
 }
 
 // ----------------------------------------------------------------------------- the tick
+constexpr int PF_RING = 64;                      // prefetched footprints in flight
+constexpr unsigned long long SPIN_CAP = 1ull << 24; // bounded waits (~seconds), then an error status
+constexpr unsigned long long SPIN_CAP_SLEEP = 1ull << 23;  // waits with a nanosleep per round
+
 struct TickSmem {
   unsigned hist[TICK_WARPS * 256];
   unsigned sred[2 * 256 + 64];
   unsigned pq[PRESS_QCAP];
   unsigned long long vis[VIS_CAP];
   int ring[3 * 16 * 16];
+  CD pf[PF_RING][7];            // prefetched footprints (self, below, up, +x, -x, +z, -z)
+  unsigned pf_ready[PF_RING];   // the cell index whose footprint a slot holds
+  int pxyz[PF_RING][4];         // the cell's coordinates and domain id
+  unsigned fwd_key[2 * FWD_CAP];
+  unsigned fwd_val[2 * FWD_CAP];
+  float fwd_part[2 * FWD_CAP];
+  unsigned consumed;            // cells the sweep has finished
+  unsigned abort;               // a wait gave up: every warp leaves the sweep
+  unsigned scan[TICK_WARPS + 1];
 };
 
 __device__ void load_ws(const Region& R, WS& W) {
@@ -142,27 +155,373 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.epoch = 1;
   W.level_round = c.level_round != 0;
   W.changed = false;
+  W.deferred = false;
+  W.nact = W.nseed = W.nchg = 0;
+  W.fwd_key = nullptr;
+  W.fwd_val = nullptr;
+  W.fwd_part = nullptr;
+  W.ft = 0;
+  W.t_wait = W.t_pull = W.t_act = W.t_write = W.t_top = W.t_pc = W.t_tail = 0;
 }
 
+// Load a cell for the prefetch ring: the grid word is read with a fence after it, pairing with
+// the sweep's fenced publication of freshly materialised bricks.
+__device__ __forceinline__ CD load_cell_acq(const Region& R, const int* ring, int x, int y, int z) {
+  CD c;
+  c.part = 0.0f;
+  c.slot = NOSLOT;
+  c.gi = 0;
+  c.mat = 0;
+  c.out = outside(R, ring, x, y, z);
+  if (c.out) return c;
+  c.gi = grid_index(R, x >> 3, y >> 3, z >> 3);
+  unsigned g = *(volatile const unsigned*)(R.grid + c.gi);
+  __threadfence_block();
+  if (g < 256u) {
+    c.mat = (unsigned char)g;
+    return c;
+  }
+  c.slot = g - 256u;
+  size_t o = (size_t)c.slot * 512u + local_index(x, y, z);
+  c.mat = R.amat[o];
+  c.part = R.avol[o];
+  return c;
+}
+
+// ----------------------------------------------------------------- CTA-wide ordered commits
+// Exclusive prefix of per-thread flags over the CTA (in thread order). Returns this thread's
+// offset; *total gets the CTA total. All threads must call.
+__device__ unsigned cta_scan(TickSmem& sm, bool f, unsigned* total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned b = __ballot_sync(FULLMASK, f);
+  if (lane == 0) sm.scan[warp] = __popc(b);
+  __syncthreads();
+  unsigned before = 0, all = 0;
+  for (int w = 0; w < TICK_WARPS; ++w) {
+    unsigned c = sm.scan[w];
+    if ((unsigned)w < warp) before += c;
+    all += c;
+  }
+  __syncthreads();
+  *total = all;
+  return before + __popc(b & lanemask_lt());
+}
+
+// First occurrence of each cell id in an event log (stamp = lowest event index).
+__device__ void stamp_first(const Region& R, const unsigned* ev, unsigned n) {
+  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) atomicMin(&R.stamp[ev[i]], i);
+  __syncthreads();
+}
+__device__ void stamp_clear(const Region& R, const unsigned* ev, unsigned n) {
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) R.stamp[ev[i]] = 0xFFFFFFFFu;
+  __syncthreads();
+}
+
+// The sweep's FluidSim::activate calls in program order (fluid.rs:292-300): a cell joins the
+// FIFO at its first activation if it was not active already.
+// Exclusive prefix of per-thread counts over the CTA (thread order); *total = the CTA sum.
+__device__ unsigned cta_scan_count(TickSmem& sm, unsigned c, unsigned* total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned u = __shfl_up_sync(FULLMASK, incl, o);
+    if (lane >= (unsigned)o) incl += u;
+  }
+  if (lane == 31) sm.scan[warp] = incl;
+  __syncthreads();
+  unsigned before = 0, all = 0;
+  for (int w = 0; w < TICK_WARPS; ++w) {
+    unsigned s = sm.scan[w];
+    if ((unsigned)w < warp) before += s;
+    all += s;
+  }
+  __syncthreads();
+  *total = all;
+  return before + incl - c;
+}
+
+// Cell o of an activation-log word: a single cell, or wake_around's order self, +x, -x, +y, -y,
+// +z, -z (fluid.rs:302-310). Returns false for cells activate() ignores (y < 0).
+__device__ __forceinline__ bool act_cell(const Region& R, unsigned word, int o, unsigned& id) {
+  const unsigned c = word & ~ACT_AROUND;
+  if (!(word & ACT_AROUND)) {
+    id = c;
+    return o == 0;
+  }
+  const unsigned px = (unsigned)R.PX, pxy = px * (unsigned)R.PY;
+  switch (o) {
+    case 0: id = c; return true;
+    case 1: id = c + 1u; return true;
+    case 2: id = c - 1u; return true;
+    case 3: id = c + px; return true;
+    case 4: id = c - px; return ((c / px) % (unsigned)R.PY) != 0u;  // y - 1 < 0
+    case 5: id = c + pxy; return true;
+    default: id = c - pxy; return true;
+  }
+}
+
+// The tick's FluidSim::activate calls in program order (fluid.rs:292-300): a cell joins the
+// FIFO at its first activation if it was not active already. Log word i covers activation
+// indices 8i..8i+6, which keeps program order for the first-occurrence stamps.
+__device__ void commit_acts(const Region& R, TickSmem& sm, unsigned n, unsigned long long& qtail, unsigned long long qhead) {
+  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) {
+    unsigned w = R.ev_act[i], id;
+    for (int o = 0; o < 7; ++o)
+      if (act_cell(R, w, o, id)) atomicMin(&R.stamp[id], i * 8u + (unsigned)o);
+  }
+  __syncthreads();
+  __shared__ unsigned long long s_tail;
+  if (threadIdx.x == 0) s_tail = qtail;
+  __syncthreads();
+  for (unsigned base = 0; base < n; base += TICK_THREADS) {
+    const unsigned i = base + threadIdx.x;
+    unsigned newmask = 0, w = 0;
+    if (i < n) {
+      w = R.ev_act[i];
+      unsigned id;
+      for (int o = 0; o < 7; ++o)
+        if (act_cell(R, w, o, id) && R.stamp[id] == i * 8u + (unsigned)o && !((R.active[id >> 5] >> (id & 31)) & 1u)) newmask |= 1u << o;
+    }
+    unsigned total;
+    unsigned off = cta_scan_count(sm, __popc(newmask), &total);
+    for (int o = 0; o < 7; ++o) {
+      if (!(newmask & (1u << o))) continue;
+      unsigned id;
+      act_cell(R, w, o, id);
+      R.queue[(s_tail + off) & R.qmask] = id;
+      atomicOr(&R.active[id >> 5], 1u << (id & 31));
+      ++off;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_tail += total;
+    __syncthreads();
+  }
+  qtail = s_tail;
+  if (threadIdx.x == 0 && s_tail - qhead > R.qmask + 1ull) set_status(R, ST_OOM, 12);
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) {
+    unsigned w = R.ev_act[i], id;
+    for (int o = 0; o < 7; ++o)
+      if (act_cell(R, w, o, id)) R.stamp[id] = 0xFFFFFFFFu;
+  }
+  __syncthreads();
+}
+
+// FluidSim::seed_level calls in order (fluid.rs:312-316): first insertion of a cell not yet a
+// seed, while the set holds fewer than MAX_LEVEL_SEEDS.
+__device__ void commit_seeds(const Region& R, TickSmem& sm, unsigned n, unsigned& nseeds) {
+  stamp_first(R, R.ev_seed, n);
+  __shared__ unsigned s_ns;
+  if (threadIdx.x == 0) s_ns = nseeds;
+  __syncthreads();
+  for (unsigned base = 0; base < n; base += TICK_THREADS) {
+    unsigned i = base + threadIdx.x;
+    bool isnew = false;
+    unsigned id = 0;
+    if (i < n) {
+      id = R.ev_seed[i];
+      isnew = R.stamp[id] == i && !((R.seedbits[id >> 5] >> (id & 31)) & 1u);
+    }
+    unsigned total;
+    unsigned off = cta_scan(sm, isnew, &total);
+    unsigned pos = s_ns + off;
+    if (isnew && pos < MAX_LEVEL_SEEDS) {
+      R.seeds[pos] = id;
+      atomicOr(&R.seedbits[id >> 5], 1u << (id & 31));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_ns = min(MAX_LEVEL_SEEDS, s_ns + total);
+    __syncthreads();
+  }
+  nseeds = s_ns;
+  stamp_clear(R, R.ev_seed, n);
+}
+
+// Voxel changes for the host (order irrelevant; the host sorts and dedups its dirty list).
+__device__ void commit_chgs(const Region& R, unsigned n) {
+  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) record_change(R, R.ev_chg[i]);
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------------ the sweep
+// Warp 0 walks the sorted cells (the reference's order); warps 1.. prefetch footprints of the
+// cells ahead into a shared-memory ring. Values the sweep wrote after a footprint was fetched
+// are taken from a forwarding table that holds every write of the last 64..128 cells.
+__device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip) {
+  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  if (tid == 0) {
+    sm.consumed = 0;
+    sm.abort = 0;
+  }
+  for (unsigned i = tid; i < PF_RING; i += TICK_THREADS) sm.pf_ready[i] = 0xFFFFFFFFu;
+  for (unsigned i = tid; i < 2 * FWD_CAP; i += TICK_THREADS) sm.fwd_key[i] = EMPTY_ID;
+  __syncthreads();
+  if (warp == 0) {
+    WS W = sW;
+    W.fwd_key = sm.fwd_key;
+    W.fwd_val = sm.fwd_val;
+    W.fwd_part = sm.fwd_part;
+    W.ft = 0;
+    Smem S{sm.vis, sm.pq, ring};
+    for (unsigned r = 0; r < n; ++r) {
+      if (r && (r & 63u) == 0u) {  // new epoch: the table of two epochs ago is reused
+        W.ft ^= 1;
+        for (int i = lane; i < FWD_CAP; i += 32) sm.fwd_key[W.ft * FWD_CAP + i] = EMPTY_ID;
+        __syncwarp();
+      }
+      const unsigned slot = r % PF_RING;
+      // wait (lane 0, bounded) for the footprint of cell r, then share the outcome
+      unsigned ok = 1u;
+      const long long tw = clock64();
+      if (lane == 0) {
+        unsigned long long spins = 0;
+        while (*(volatile unsigned*)&sm.pf_ready[slot] != r) {
+          if (++spins > SPIN_CAP_SLEEP) {
+            ok = 0u;
+            break;
+          }
+          __nanosleep(20);
+        }
+        __threadfence_block();
+      }
+      ok = __shfl_sync(FULLMASK, ok, 0);
+      W.t_wait += clock64() - tw;
+      if (!ok) {
+        if (lane == 0) {
+          set_status(R, ST_TIMEOUT, 20);
+          *(volatile unsigned*)&sm.abort = 1u;
+        }
+        break;
+      }
+      __syncwarp();
+      __threadfence_block();
+      const int x = sm.pxyz[slot][0], y = sm.pxyz[slot][1], z = sm.pxyz[slot][2];
+      const unsigned cid = (unsigned)sm.pxyz[slot][3];
+      if (lane < 7) {
+        CD mine = sm.pf[slot][lane];
+        if (!mine.out) {
+          const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
+          const unsigned fid = lane == 0 ? cid : lane == 1 ? cid - (unsigned)R.PX : lane == 2 ? cid + (unsigned)R.PX
+                             : lane == 3 ? cid + 1u : lane == 4 ? cid - 1u : lane == 5 ? cid + pxy : cid - pxy;
+          unsigned char m;
+          float p;
+          if (fwd_lookup_t(W, W.ft, fid, m, p) || fwd_lookup_t(W, W.ft ^ 1, fid, m, p)) {
+            mine.mat = m;
+            mine.part = p;
+            // a brick materialised since the fetch: take the slot now
+            if (mine.slot == NOSLOT) {
+              unsigned g = R.grid[mine.gi];
+              if (g >= 256u) mine.slot = g - 256u;
+            }
+            sm.pf[slot][lane] = mine;
+          }
+        }
+      }
+      __syncwarp();
+      const long long t1 = clock64();
+      W.t_top += t1 - tw;
+      process_cell(R, W, S, x, y, z, sm.pf[slot]);
+      __syncwarp();
+      const long long t2 = clock64();
+      W.t_pc += t2 - t1;
+      __threadfence_block();
+      if (lane == 0) *(volatile unsigned*)&sm.consumed = r + 1u;
+      W.t_tail += clock64() - t2;
+    }
+    W.fwd_key = nullptr;
+    W.fwd_val = nullptr;
+    W.fwd_part = nullptr;
+    long long pd = W.pdelta;  // lane-local partial-count deltas
+    for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
+    W.pdelta = pd;
+    if (lane == 0) {
+      sW = W;
+      Ctl& c = *R.ctl;
+      c.prof[3] += W.t_wait;
+      c.prof[4] += W.t_pull;
+      c.prof[5] += W.t_act;
+      c.prof[6] += W.t_write;
+      c.prof[12] += W.t_top;
+      c.prof[13] += W.t_pc;
+      c.prof[14] += W.t_tail;
+      sW.t_wait = sW.t_pull = sW.t_act = sW.t_write = sW.t_top = sW.t_pc = sW.t_tail = 0;
+    }
+    __syncwarp();
+  } else {
+    // producers: warp p prefetches cells p-1, p-1+NP, ...
+    const unsigned NP = TICK_WARPS - 1;
+    for (unsigned r = warp - 1; r < n; r += NP) {
+      // wait (lane 0, bounded) until the ring slot of cell r is free
+      unsigned ok = 1u;
+      if (lane == 0) {
+        unsigned long long spins = 0;
+        while (*(volatile unsigned*)&sm.consumed + PF_RING <= r) {
+          if (*(volatile unsigned*)&sm.abort || ++spins > SPIN_CAP_SLEEP) {
+            ok = 0u;
+            break;
+          }
+          __nanosleep(200);  // yield issue slots to the sweep warp
+        }
+        __threadfence_block();
+      }
+      ok = __shfl_sync(FULLMASK, ok, 0);
+      if (!ok) break;
+      __syncwarp();
+      __threadfence_block();
+      int x, y, z;
+      const unsigned cid = key_to_id(R, R.cells[r], flip);
+      dom_xyz(R, cid, x, y, z);
+      if (lane < 7) {
+        int fx = x + (lane == 3) - (lane == 4), fy = y - (lane == 1) + (lane == 2), fz = z + (lane == 5) - (lane == 6);
+        sm.pf[r % PF_RING][lane] = load_cell_acq(R, ring, fx, fy, fz);
+      } else if (lane == 7) {
+        sm.pxyz[r % PF_RING][0] = x;
+        sm.pxyz[r % PF_RING][1] = y;
+        sm.pxyz[r % PF_RING][2] = z;
+        sm.pxyz[r % PF_RING][3] = (int)cid;
+      }
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) *(volatile unsigned*)&sm.pf_ready[r % PF_RING] = r;
+    }
+  }
+  __syncthreads();
+}
 // FluidSim::tick (fluid.rs:564-657) for region R, n_ticks times. All threads of the CTA enter.
+// Per tick: drain the FIFO head and sort it (CTA), the sweep (warp 0, prefetched by the other
+// warps), the seed log's commit, levelling (warp 0), then the activation and change logs'
+// commits (CTA). The logs keep program order, so the committed FIFO and seed list are exactly
+// the reference's.
 __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
   const unsigned tid = threadIdx.x, warp = tid >> 5;
-  // ring table to shared memory when small
   const int* ring = R.ring;
   if (R.ring_w && R.ring_w <= 16) {
     for (int i = tid; i < 3 * R.ring_w * R.ring_w; i += TICK_THREADS) sm.ring[i] = R.ring[i];
     ring = sm.ring;
   }
   for (unsigned i = tid; i < VIS_CAP; i += TICK_THREADS) sm.vis[i] = 0ull;
-  __shared__ unsigned s_n, s_flip, s_clear, s_abort;
+  __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds;
+  __shared__ unsigned long long s_qtail;
   __shared__ WS sW;
   if (tid == 0) {
     load_ws(R, sW);
+    sW.deferred = true;
     s_abort = R.ctl->status != 0;
+    s_clear = 0;
   }
   __syncthreads();
+  long long tp = clock64();
+  auto lap = [&](int k) {
+    if (tid == 0) {
+      long long now = clock64();
+      R.ctl->prof[k] += (unsigned long long)(now - tp);
+      tp = now;
+    }
+  };
   for (int t = 0; t < n_ticks; ++t) {
     if (s_abort) break;
+    lap(15);
     // ---- drain the FIFO head (fluid.rs:565-572)
     if (tid == 0) {
       unsigned tick = R.ctl->tick_no + 1u;
@@ -181,53 +540,80 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
       R.cells[i] = sort_key(R, id, flip);
     }
     __syncthreads();
-    if (tid == 0) sW.qhead = qh + n;
+    if (tid == 0) {
+      sW.qhead = qh + n;
+      sW.pulls = 0;
+      sW.changed = false;
+      sW.activations = sW.pull_attempts = sW.pull_success = sW.bfs_visits = sW.level_cells_total = 0;
+      sW.pdelta = 0;
+      sW.nact = sW.nseed = sW.nchg = 0;
+    }
     __syncthreads();
+    lap(0);
     // ---- sort (fluid.rs:575-580)
     cta_radix_sort(R.cells, R.cells_tmp, n, sm.hist, sm.sred);
-    // ---- the sweep (fluid.rs:584-651), one warp, reference order
+    __syncthreads();
+    lap(1);
+    // ---- the sweep (fluid.rs:584-651)
+    sweep(R, sm, sW, ring, n, flip);
+    lap(2);
+    if (sm.abort) {
+      if (tid == 0) s_abort = 1;
+      __syncthreads();
+      break;
+    }
+    // ---- level seeds logged by the sweep (fluid.rs:312-316)
+    if (tid == 0) s_nseeds = sW.nseeds;
+    __syncthreads();
+    unsigned nseeds = s_nseeds;
+    commit_seeds(R, sm, min(sW.nseed, R.ev_seed_cap), nseeds);
+    if (tid == 0) sW.nseeds = nseeds;
+    __syncthreads();
+    lap(7);
+    // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      W.pulls = 0;
-      W.changed = false;
-      W.activations = W.pull_attempts = W.pull_success = W.bfs_visits = W.level_cells_total = 0;
-      W.pdelta = 0;
       Smem S{sm.vis, sm.pq, ring};
-      for (unsigned r = 0; r < n; ++r) {
-        unsigned id = key_to_id(R, R.cells[r], flip);
-        int x, y, z;
-        dom_xyz(R, id, x, y, z);
-        process_cell(R, W, S, x, y, z);
-      }
-      // ---- levelling (fluid.rs:652-655)
+      W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
-      // partial_count delta: reduce across lanes
       long long pd = W.pdelta;
       for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
       if (lane_id() == 0) {
-        Ctl& c = *R.ctl;
-        c.last_cells = n;
-        c.cells_total += n;
-        c.pull_attempts += W.pull_attempts;
-        c.pull_success += W.pull_success;
-        c.bfs_visits += W.bfs_visits;
-        c.level_cells_total += W.level_cells_total;
-        c.activations += W.activations;
-        c.partial_count += pd;
-        c.last_level_cells = W.llc;
-        c.nseeds = W.nseeds;
-        c.level_round = W.level_round ? 1u : 0u;
-        if (W.changed) c.changed = 1u;
-        c.qhead = W.qhead;
-        c.qtail = W.qtail;
-        W.pdelta = 0;
+        W.pdelta = sW.pdelta + pd;
         sW = W;
-        sW.pdelta = 0;
         s_clear = clear;
-        s_abort = c.status != 0;
       }
       __syncwarp();
+    }
+    __syncthreads();
+    lap(8);
+    // ---- FIFO appends and voxel changes logged during the tick
+    if (tid == 0) s_qtail = sW.qtail;
+    __syncthreads();
+    unsigned long long qt = s_qtail;
+    commit_acts(R, sm, min(sW.nact, R.ev_act_cap), qt, sW.qhead);
+    lap(9);
+    commit_chgs(R, min(sW.nchg, R.ev_chg_cap));
+    lap(10);
+    if (tid == 0) {
+      Ctl& c = *R.ctl;
+      c.activations += qt - s_qtail;
+      sW.qtail = qt;
+      c.last_cells = n;
+      c.cells_total += n;
+      c.pull_attempts += sW.pull_attempts;
+      c.pull_success += sW.pull_success;
+      c.bfs_visits += sW.bfs_visits;
+      c.level_cells_total += sW.level_cells_total;
+      c.partial_count += sW.pdelta;
+      c.last_level_cells = sW.llc;
+      c.nseeds = sW.nseeds;
+      c.level_round = sW.level_round ? 1u : 0u;
+      if (sW.changed) c.changed = 1u;
+      c.qhead = sW.qhead;
+      c.qtail = sW.qtail;
+      s_abort = c.status != 0;
     }
     __syncthreads();
     // ---- end of a levelling round: clear the marks it touched (fluid.rs:503-505)
@@ -239,9 +625,13 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
         if (lane_id() == 0) R.mark_tflag[tile] = 0u;
       }
       __syncthreads();
-      if (tid == 0) R.ctl->mark_ntiles = 0;
+      if (tid == 0) {
+        R.ctl->mark_ntiles = 0;
+        s_clear = 0;
+      }
       __syncthreads();
     }
+    lap(11);
   }
 }
 
