@@ -154,6 +154,31 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
  * 15 between ticks. */
 int vf_fluid_profile(vf_fluid* h, uint64_t* out16);
 
+/* Launch knobs of the tick (the autotuner's search space; results never depend on them):
+ * warps prefetching footprints (1..7) and how many cells ahead of the sweep they run (1..64). */
+int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
+
+/* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
+ * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */
+int vf_fluid_emit_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, float amount);
+int vf_fluid_brush_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, uint8_t m);
+int vf_fluid_wake_async(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1);
+
+/* A batch: many regions stepped by one launch, one CTA per region, on hs[0]'s stream.
+ * vf_batch_capture records `launches` launches of `ticks_per_launch` ticks as a CUDA graph that
+ * vf_batch_replay relaunches; vf_batch_sync waits and checks every region's status. */
+typedef struct vf_batch vf_batch;
+int vf_batch_create(vf_fluid* const* hs, int32_t n, vf_batch** out);
+void vf_batch_destroy(vf_batch* b);
+int vf_batch_tick_async(vf_batch* b, int32_t n_ticks);
+int vf_batch_sync(vf_batch* b);
+int vf_batch_capture(vf_batch* b, int32_t launches, int32_t ticks_per_launch);
+int vf_batch_replay(vf_batch* b);
+/* Record everything enqueued on the batch's stream between these two calls (tick launches,
+ * device edits, wakes; every handle must run on the batch's stream) as the graph to replay. */
+int vf_batch_begin_capture(vf_batch* b);
+int vf_batch_end_capture(vf_batch* b);
+
 /* ---- batched regions: pattern (2) of the engine. Every handle is an independent FluidSim
  * (its own world, FIFO, caps); one launch steps all of them n_ticks times, one CTA per region.
  * All handles must live on the same device; the launch runs on hs[0]'s stream. */

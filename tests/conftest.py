@@ -10,6 +10,8 @@ sys.path.insert(0, str(ROOT))
 
 import __graft_entry__ as ge  # noqa: E402
 
+ge.load_package()  # importable as `vfwater` (and `vfwater.runner`) in every test module
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")

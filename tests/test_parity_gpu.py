@@ -204,3 +204,59 @@ def test_partials_export_and_set_partial(vf, orc):
         sim.tick()
         o.tick()
         assert_same_digest(sim, o, t + 1)
+
+
+def _oracle_script(wl, oracles, t0, ticks):
+    for t in range(t0, t0 + ticks):
+        for r, o in enumerate(oracles):
+            if wl.emit_every and t % wl.emit_every == 0:
+                em, amt = wl.emitters(r)
+                if len(em):
+                    o.emit(em, amt)
+            if wl.edit_every and t % wl.edit_every == wl.edit_every - 1:
+                ed = wl.edit(r, t)
+                if ed is not None:
+                    cells, m, wake = ed
+                    o.apply_brush(cells, m)
+                    o.wake(*map(int, wake))
+            o.tick()
+
+
+@pytest.mark.parametrize("wid,scale,ticks", [(4, 0.12, 24), (5, 0.05, 40), (3, 0.06, 30)])
+def test_batched_graph_script_matches_oracle(vf, orc, wid, scale, ticks):
+    """One CUDA graph over all regions (ticks, device-side emitters / brushes / wakes) equals the
+    oracle running the same script."""
+    import torch
+
+    from vfwater import runner
+
+    stream = torch.cuda.Stream()
+    wl = vf.Workload(wid, scale, 3)
+    sims = runner.make_sims(vf, wl, stream.cuda_stream)
+    oracles = []
+    for r in range(wl.regions):
+        o = oracle_for(orc, wl.world(r))
+        for b in wl.wakes(r):
+            o.wake(*map(int, b))
+        oracles.append(o)
+    res = runner.run_batched(vf, wl, sims, 0, ticks, torch, stream)
+    _oracle_script(wl, oracles, 0, ticks)
+    assert res.cells == sum(o.stats()["cells"] for o in oracles)
+    for s, o in zip(sims, oracles):
+        assert_same_digest(s, o, ticks)
+
+
+def test_plain_and_batched_modes_agree(vf):
+    import torch
+
+    from vfwater import runner
+
+    stream = torch.cuda.Stream()
+    wl = vf.Workload(5, 0.05, 9)
+    a = runner.make_sims(vf, wl, stream.cuda_stream)
+    b = runner.make_sims(vf, wl, stream.cuda_stream, tune=(2, 16))
+    ra = runner.run_plain(vf, wl, a, 0, 25, torch, stream)
+    rb = runner.run_batched(vf, wl, b, 0, 25, torch, stream)
+    assert ra.cells == rb.cells
+    for x, y in zip(a, b):
+        assert x.digest() == y.digest()

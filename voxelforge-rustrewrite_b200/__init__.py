@@ -152,6 +152,18 @@ def lib():
         "vf_fluid_digest": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vf_fluid_batch_tick": (C.c_int, [C.POINTER(P), I32, I32]),
         "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+        "vf_fluid_set_tuning": (C.c_int, [P, I32, I32]),
+        "vf_fluid_emit_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_float]),
+        "vf_fluid_brush_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_uint8]),
+        "vf_fluid_wake_async": (C.c_int, [P, I32, I32, I32, I32, I32, I32]),
+        "vf_batch_create": (C.c_int, [C.POINTER(P), I32, C.POINTER(P)]),
+        "vf_batch_destroy": (None, [P]),
+        "vf_batch_tick_async": (C.c_int, [P, I32]),
+        "vf_batch_sync": (C.c_int, [P]),
+        "vf_batch_capture": (C.c_int, [P, I32, I32]),
+        "vf_batch_replay": (C.c_int, [P]),
+        "vf_batch_begin_capture": (C.c_int, [P]),
+        "vf_batch_end_capture": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -362,6 +374,19 @@ class FluidSim:
         self._check(lib().vf_fluid_tick(self.h, n, C.byref(ch)), "tick")
         return bool(ch.value)
 
+    def set_tuning(self, producers: int, depth: int):
+        """Launch knobs (prefetch warps, prefetch distance); results never depend on them."""
+        self._check(lib().vf_fluid_set_tuning(self.h, producers, depth), "set_tuning")
+
+    def emit_device_async(self, dev_xyz_ptr: int, n: int, amount: float):
+        self._check(lib().vf_fluid_emit_device_async(self.h, C.c_void_p(dev_xyz_ptr), n, amount), "emit_device_async")
+
+    def brush_device_async(self, dev_xyz_ptr: int, n: int, m: int):
+        self._check(lib().vf_fluid_brush_device_async(self.h, C.c_void_p(dev_xyz_ptr), n, m), "brush_device_async")
+
+    def wake_async(self, x0, y0, z0, x1, y1, z1):
+        self._check(lib().vf_fluid_wake_async(self.h, x0, y0, z0, x1, y1, z1), "wake_async")
+
     def tick_async(self, n: int = 1):
         """Enqueue n ticks on the handle's stream without waiting."""
         self._check(lib().vf_fluid_tick_async(self.h, n), "tick_async")
@@ -497,6 +522,49 @@ class FluidSim:
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
         self._check(lib().vf_fluid_digest(self.h, C.byref(a), C.byref(b), C.byref(c)), "digest")
         return a.value, b.value, c.value
+
+
+class Batch:
+    """Many independent FluidSims stepped by one launch (one CTA per region), optionally as a
+    captured CUDA graph. All sims must share a device; the batch runs on the first sim's stream."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (P * len(self.sims))(*[s.h.value for s in self.sims])
+        h = P()
+        rc = lib().vf_batch_create(arr, len(self.sims), C.byref(h))
+        if rc:
+            raise VfError(rc, "vf_batch_create", (lib().vf_fluid_last_error(self.sims[0].h) or b"").decode())
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc:
+            raise VfError(rc, what, (lib().vf_fluid_last_error(self.sims[0].h) or b"").decode())
+
+    def tick_async(self, n: int):
+        self._check(lib().vf_batch_tick_async(self.h, n), "batch_tick_async")
+
+    def sync(self):
+        self._check(lib().vf_batch_sync(self.h), "batch_sync")
+
+    def capture(self, launches: int, ticks_per_launch: int):
+        self._check(lib().vf_batch_capture(self.h, launches, ticks_per_launch), "batch_capture")
+
+    def replay(self):
+        self._check(lib().vf_batch_replay(self.h), "batch_replay")
+
+    def begin_capture(self):
+        self._check(lib().vf_batch_begin_capture(self.h), "batch_begin_capture")
+
+    def end_capture(self):
+        self._check(lib().vf_batch_end_capture(self.h), "batch_end_capture")
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.vf_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
 
 
 def batch_tick(sims, n_ticks: int):

@@ -33,6 +33,16 @@ struct vf_fluid {
   size_t scratch_bytes = 0;
   // tick launch shape
   int smem_bytes = 0;
+  Tune tune{TICK_WARPS - 1, PF_RING};
+};
+
+// A set of regions stepped together: one CTA per region in one launch (pattern (2)).
+struct vf_batch {
+  std::vector<vf_fluid*> hs;
+  Region* dregs = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
@@ -380,7 +390,7 @@ int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks) {
   h->hzero[0] = 0u;
   CK(cudaMemcpyAsync(&h->R.ctl->changed, h->hzero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
   if (n_ticks > 0) {
-    k_tick<<<1, TICK_THREADS, h->smem_bytes, h->stream>>>(h->dR, 1, n_ticks);
+    k_tick<<<1, TICK_THREADS, h->smem_bytes, h->stream>>>(h->dR, 1, n_ticks, h->tune);
     CK(cudaGetLastError());
   }
   return VF_OK;
@@ -678,6 +688,153 @@ int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
   return VF_OK;
 }
 
+int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
+  if (!h || producers < 1 || producers > TICK_WARPS - 1 || depth < 1 || depth > PF_RING) return VF_ERR_INVALID;
+  h->tune = Tune{producers, depth};
+  return VF_OK;
+}
+
+// Host edits that take their cell list from DEVICE memory and do not wait: capturable in a
+// CUDA graph together with vf_batch_tick_async / vf_fluid_tick_async.
+int vf_fluid_emit_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, float amount) {
+  int rc = check(h);
+  if (rc) return rc;
+  k_edit<<<1, 32, 0, h->stream>>>(h->R, ED_EMIT, dev_xyz, n, 0, amount, nullptr);
+  CK(cudaGetLastError());
+  return VF_OK;
+}
+
+int vf_fluid_brush_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, uint8_t m) {
+  int rc = check(h);
+  if (rc) return rc;
+  k_edit<<<1, 32, 0, h->stream>>>(h->R, ED_BRUSH, dev_xyz, n, m, 0.0f, nullptr);
+  CK(cudaGetLastError());
+  return VF_OK;
+}
+
+int vf_fluid_wake_async(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (x1 < x0 || y1 < y0 || z1 < z0) return VF_OK;
+  y0 = std::max(y0, 0);
+  if (y1 < y0) return VF_OK;
+  if (!in_dom(h->R, x0, y0, z0) || !in_dom(h->R, x1, y1, z1)) return fail(h, VF_ERR_RANGE, "wake box outside the padded domain");
+  k_wake_box<<<1, 1024, 0, h->stream>>>(h->R, x0, y0, z0, x1, y1, z1);
+  CK(cudaGetLastError());
+  return VF_OK;
+}
+
+int vf_batch_create(vf_fluid* const* hs, int32_t n, vf_batch** out) {
+  if (!hs || n <= 0 || !out) return VF_ERR_INVALID;
+  vf_fluid* h = hs[0];
+  for (int i = 0; i < n; ++i) {
+    int rc = check(hs[i]);
+    if (rc) return rc;
+    if (hs[i]->device != h->device) return fail(h, VF_ERR_INVALID, "batched handles must share a device");
+  }
+  auto* b = new vf_batch();
+  b->hs.assign(hs, hs + n);
+  b->stream = h->stream;
+  std::vector<Region> regs(n);
+  for (int i = 0; i < n; ++i) regs[i] = hs[i]->R;
+  if (cudaMalloc(&b->dregs, sizeof(Region) * n) != cudaSuccess) {
+    delete b;
+    return VF_ERR_OOM;
+  }
+  if (cudaMemcpy(b->dregs, regs.data(), sizeof(Region) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(b->dregs);
+    delete b;
+    return VF_ERR_CUDA;
+  }
+  *out = b;
+  return VF_OK;
+}
+
+void vf_batch_destroy(vf_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->dregs) cudaFree(b->dregs);
+  delete b;
+}
+
+int vf_batch_tick_async(vf_batch* b, int32_t n_ticks) {
+  if (!b || n_ticks < 0) return VF_ERR_INVALID;
+  vf_fluid* h = b->hs[0];
+  if (n_ticks) {
+    k_tick<<<(unsigned)b->hs.size(), TICK_THREADS, h->smem_bytes, b->stream>>>(b->dregs, (int)b->hs.size(), n_ticks, h->tune);
+    CK(cudaGetLastError());
+  }
+  return VF_OK;
+}
+
+int vf_batch_sync(vf_batch* b) {
+  if (!b) return VF_ERR_INVALID;
+  vf_fluid* h = b->hs[0];
+  CK(cudaStreamSynchronize(b->stream));
+  for (vf_fluid* x : b->hs) {
+    int rc = sync_ctl(x);
+    if (rc) return rc;
+  }
+  return VF_OK;
+}
+
+// Capture `launches` back-to-back launches of `ticks_per_launch` ticks each into a CUDA graph.
+int vf_batch_capture(vf_batch* b, int32_t launches, int32_t ticks_per_launch) {
+  if (!b || launches <= 0 || ticks_per_launch <= 0) return VF_ERR_INVALID;
+  vf_fluid* h = b->hs[0];
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < launches; ++i)
+    k_tick<<<(unsigned)b->hs.size(), TICK_THREADS, h->smem_bytes, b->stream>>>(b->dregs, (int)b->hs.size(), ticks_per_launch, h->tune);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+  if (e != cudaSuccess) return fail(h, VF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return VF_OK;
+}
+
+// Record everything enqueued on the batch's stream between these calls (tick launches, device
+// edits, wakes of the batch's handles) as one CUDA graph for vf_batch_replay.
+int vf_batch_begin_capture(vf_batch* b) {
+  if (!b) return VF_ERR_INVALID;
+  vf_fluid* h = b->hs[0];
+  for (vf_fluid* x : b->hs)
+    if (x->stream != b->stream) return fail(h, VF_ERR_INVALID, "capture needs every handle on the batch's stream");
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  return VF_OK;
+}
+
+int vf_batch_end_capture(vf_batch* b) {
+  if (!b) return VF_ERR_INVALID;
+  vf_fluid* h = b->hs[0];
+  cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+  if (e != cudaSuccess) return fail(h, VF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return VF_OK;
+}
+
+int vf_batch_replay(vf_batch* b) {
+  if (!b || !b->exec) return VF_ERR_STATE;
+  vf_fluid* h = b->hs[0];
+  CK(cudaGraphLaunch(b->exec, b->stream));
+  return VF_OK;
+}
+
 // ------------------------------------------------------------------------ batched regions
 int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks) {
   if (!hs || n <= 0 || n_ticks < 0) return VF_ERR_INVALID;
@@ -694,7 +851,7 @@ int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks) {
   CK(cudaMemcpyAsync(h->scratch, regs.data(), sizeof(Region) * n, cudaMemcpyHostToDevice, h->stream));
   for (int i = 0; i < n; ++i) CK(cudaMemsetAsync(&regs[i].ctl->changed, 0, 4, h->stream));
   if (n_ticks) {
-    k_tick<<<n, TICK_THREADS, h->smem_bytes, h->stream>>>((Region*)h->scratch, n, n_ticks);
+    k_tick<<<n, TICK_THREADS, h->smem_bytes, h->stream>>>((Region*)h->scratch, n, n_ticks, h->tune);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(h->stream));

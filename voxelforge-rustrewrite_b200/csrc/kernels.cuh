@@ -119,6 +119,13 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
 
 // ----------------------------------------------------------------------------- the tick
 constexpr int PF_RING = 64;                      // prefetched footprints in flight
+
+// Launch-time knobs of the tick (chosen by the autotuner; results do not depend on them):
+// producer warps prefetching footprints and how far ahead of the sweep they may run.
+struct Tune {
+  int producers;  // 1 .. TICK_WARPS-1
+  int depth;      // 1 .. PF_RING
+};
 constexpr unsigned long long SPIN_CAP = 1ull << 24; // bounded waits (~seconds), then an error status
 constexpr unsigned long long SPIN_CAP_SLEEP = 1ull << 23;  // waits with a nanosleep per round
 
@@ -348,7 +355,7 @@ __device__ void commit_chgs(const Region& R, unsigned n) {
 // Warp 0 walks the sorted cells (the reference's order); warps 1.. prefetch footprints of the
 // cells ahead into a shared-memory ring. Values the sweep wrote after a footprint was fetched
 // are taken from a forwarding table that holds every write of the last 64..128 cells.
-__device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip) {
+__device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   if (tid == 0) {
     sm.consumed = 0;
@@ -448,15 +455,16 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       sW.t_wait = sW.t_pull = sW.t_act = sW.t_write = sW.t_top = sW.t_pc = sW.t_tail = 0;
     }
     __syncwarp();
-  } else {
+  } else if (warp <= (unsigned)tune.producers) {
     // producers: warp p prefetches cells p-1, p-1+NP, ...
-    const unsigned NP = TICK_WARPS - 1;
+    const unsigned NP = (unsigned)tune.producers;
+    const unsigned depth = (unsigned)tune.depth;
     for (unsigned r = warp - 1; r < n; r += NP) {
       // wait (lane 0, bounded) until the ring slot of cell r is free
       unsigned ok = 1u;
       if (lane == 0) {
         unsigned long long spins = 0;
-        while (*(volatile unsigned*)&sm.consumed + PF_RING <= r) {
+        while (*(volatile unsigned*)&sm.consumed + depth <= r) {
           if (*(volatile unsigned*)&sm.abort || ++spins > SPIN_CAP_SLEEP) {
             ok = 0u;
             break;
@@ -493,7 +501,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
 // warps), the seed log's commit, levelling (warp 0), then the activation and change logs'
 // commits (CTA). The logs keep program order, so the committed FIFO and seed list are exactly
 // the reference's.
-__device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
+__device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune) {
   const unsigned tid = threadIdx.x, warp = tid >> 5;
   const int* ring = R.ring;
   if (R.ring_w && R.ring_w <= 16) {
@@ -555,7 +563,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
     __syncthreads();
     lap(1);
     // ---- the sweep (fluid.rs:584-651)
-    sweep(R, sm, sW, ring, n, flip);
+    sweep(R, sm, sW, ring, n, flip, tune);
     lap(2);
     if (sm.abort) {
       if (tid == 0) s_abort = 1;
@@ -635,11 +643,11 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks) {
   }
 }
 
-__global__ void __launch_bounds__(TICK_THREADS, 1) k_tick(Region* regs, int nreg, int n_ticks) {
+__global__ void __launch_bounds__(TICK_THREADS, 1) k_tick(Region* regs, int nreg, int n_ticks, Tune tune) {
   extern __shared__ __align__(16) unsigned char smraw[];
   TickSmem& sm = *reinterpret_cast<TickSmem*>(smraw);
   for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
-    run_ticks(regs[r], sm, n_ticks);
+    run_ticks(regs[r], sm, n_ticks, tune);
     __syncthreads();
   }
 }
