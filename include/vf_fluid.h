@@ -154,6 +154,27 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
  * 15 between ticks. */
 int vf_fluid_profile(vf_fluid* h, uint64_t* out16);
 
+/* ---- learned wake proposal (pattern (4)). Rows are atlas slots (materialised bricks).
+ * Features: nslots x 32 fp16 into device memory (advances a 4-call history: call once per tick).
+ * Labels: 1.0 where the brick's cells were drained in (since_tick, now]. Staging: L2 prefetch of
+ * the bricks whose probability >= threshold; it never changes what the fluid computes. */
+int vf_fluid_proposal_features(vf_fluid* h, void* dev_x_f16, uint64_t cap_slots, uint64_t* nslots);
+int vf_fluid_proposal_labels(vf_fluid* h, uint32_t since_tick, float* dev_y, uint64_t nslots);
+int vf_fluid_stage_bricks(vf_fluid* h, const float* dev_prob, uint64_t nslots, float threshold, uint64_t* n_staged);
+
+/* The proposal network: 32 -> 64 -> 64 -> 1 (ReLU, ReLU, sigmoid), fp16 tensor-core forward and
+ * backward kernels, fp32 master weights, Adam. All tensors are device pointers; flat fp32
+ * parameters: W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3. */
+typedef struct vf_mlp vf_mlp;
+int vf_mlp_create(int32_t device, uint64_t seed, vf_mlp** out);
+void vf_mlp_destroy(vf_mlp* m);
+int vf_mlp_nparams(void);
+int vf_mlp_get_params(vf_mlp* m, float* host_out);
+int vf_mlp_set_params(vf_mlp* m, const float* host_in);
+int vf_mlp_forward(vf_mlp* m, const void* dev_x_f16, uint64_t n, float* dev_prob, void* stream);
+int vf_mlp_grads(vf_mlp* m, const void* dev_x_f16, const float* dev_y, uint64_t n, float* host_grads, void* stream);
+int vf_mlp_train_step(vf_mlp* m, const void* dev_x_f16, const float* dev_y, uint64_t n, float lr, float* host_loss, void* stream);
+
 /* Launch knobs of the tick (the autotuner's search space; results never depend on them):
  * warps prefetching footprints (1..7) and how many cells ahead of the sweep they run (1..64). */
 int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);

@@ -1,0 +1,89 @@
+"""The learned wake proposal: fp16 tensor-core forward/backward kernels against an fp64 CPU
+restatement, GPU training on traces of the exact engine, and the proposal never changing state."""
+import numpy as np
+import pytest
+
+from conftest import assert_same_digest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mlp_forward_and_gradients_match_fp64_reference(vf):
+    import torch
+
+    from vfwater import proposal
+
+    mlp = proposal.MLP(seed=3)
+    rng = np.random.default_rng(0)
+    n = 333  # ragged: not a multiple of the 16-row tiles
+    x = rng.normal(0, 1, size=(n, 32)).astype(np.float16)
+    y = (rng.random(n) < 0.3).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.from_numpy(y).cuda()
+    p = mlp.params()
+    # the kernels use fp16 copies of the weights: compare against the same rounding
+    p16 = p.copy()
+    p16[0:2048] = p[0:2048].astype(np.float16).astype(np.float32)
+    p16[2112:6208] = p[2112:6208].astype(np.float16).astype(np.float32)
+    prob_ref, g_ref, _ = proposal.reference_forward_backward(p16, x.astype(np.float32), y)
+    prob = mlp.forward(xd, torch).cpu().numpy()
+    assert np.allclose(prob, prob_ref, atol=5e-3), np.abs(prob - prob_ref).max()
+    g = mlp.grads(xd, yd)
+    # fp16 hidden activations: 3% of the gradient's scale
+    for lo, hi, name in [(0, 2048, "W1"), (2048, 2112, "b1"), (2112, 6208, "W2"), (6208, 6272, "b2"), (6272, 6336, "w3"), (6336, 6337, "b3")]:
+        ref, got = g_ref[lo:hi], g[lo:hi]
+        scale = np.abs(ref).max() + 1e-12
+        assert np.abs(got - ref).max() <= 0.03 * scale, f"{name}: {np.abs(got - ref).max()} vs scale {scale}"
+    mlp.close()
+
+
+def test_mlp_learns_a_separable_rule(vf):
+    import torch
+
+    from vfwater import proposal
+
+    rng = np.random.default_rng(1)
+    x = rng.normal(0, 1, size=(20000, 32)).astype(np.float16)
+    y = ((x[:, 0].astype(np.float32) + 0.5 * x[:, 3].astype(np.float32)) > 0.3).astype(np.float32)
+    X, Y = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    mlp = proposal.MLP(seed=2)
+    losses = proposal.train(mlp, X, Y, torch, epochs=6, batch=2048, lr=3e-3)
+    s = proposal.score(mlp.forward(X, torch), Y)
+    assert losses[-1] < losses[0] * 0.5
+    assert s.recall > 0.9 and s.precision > 0.9, s
+    mlp.close()
+
+
+def test_proposal_on_engine_traces_beats_persistence_and_keeps_state_exact(vf):
+    import torch
+
+    from vfwater import proposal
+
+    X, Y, B = proposal.collect(vf, torch, [(1, 1.0, 1, 10, 60, 1), (3, 0.08, 2, 5, 40, 4)], every=2)
+    assert X.shape[0] == Y.shape[0] > 1000
+    n = X.shape[0]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    perm = torch.randperm(n, device="cuda", generator=g)
+    tr, te = perm[: int(0.8 * n)], perm[int(0.8 * n):]
+    mlp = proposal.MLP(seed=5)
+    proposal.train(mlp, X[tr].contiguous(), Y[tr].contiguous(), torch, epochs=8, batch=4096, lr=2e-3)
+    s = proposal.score(mlp.forward(X[te].contiguous(), torch), Y[te])
+    base = proposal.score(B[te], Y[te])
+    # the network finds more of the bricks that wake than "it woke last tick" at useful precision
+    assert s.recall > base.recall, (s, base)
+    assert s.precision > 0.5, s
+    # staging the proposal's bricks changes nothing the fluid computes
+    wl = vf.Workload(1)
+    a, b = vf.FluidSim(wl.world(0)), vf.FluidSim(wl.world(0))
+    for sim in (a, b):
+        for box in wl.wakes(0):
+            sim.wake(*map(int, box))
+    for t in range(40):
+        x, nsl = proposal.features(b, torch)
+        if nsl:
+            proposal.stage(b, mlp.forward(x.contiguous(), torch), 0.5)
+        a.tick()
+        b.tick()
+    assert a.digest() == b.digest()
+    mlp.close()

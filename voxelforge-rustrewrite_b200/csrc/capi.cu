@@ -34,6 +34,12 @@ struct vf_fluid {
   // tick launch shape
   int smem_bytes = 0;
   Tune tune{TICK_WARPS - 1, PF_RING};
+  // wake proposal state (allocated on first use)
+  int* slot_gi = nullptr;
+  SlotAggr* aggr = nullptr;
+  float* whist = nullptr;
+  unsigned* staged = nullptr;
+  unsigned hpos = 0;
 };
 
 // A set of regions stepped together: one CTA per region in one launch (pattern (2)).
@@ -285,6 +291,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.ev_seed, R.ev_seed_cap, false))) return rc;
   if ((rc = dalloc(h, &R.ev_chg, R.ev_chg_cap, false))) return rc;
   if ((rc = dalloc(h, &R.stamp, ncells, false))) return rc;
+  if ((rc = dalloc(h, &R.last_woken, cap))) return rc;
   CK(cudaMemsetAsync(R.stamp, 0xFF, ncells * 4, h->stream));
   R.chg_cap = 1u << 22;
   if ((rc = dalloc(h, &R.chg, R.chg_cap, false))) return rc;
@@ -685,6 +692,73 @@ int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
   if (out16) std::memcpy(out16, h->hctl->prof, sizeof(h->hctl->prof));
+  return VF_OK;
+}
+
+// ---------------------------------------------------------------- learned wake proposal
+static int proposal_buffers(vf_fluid* h) {
+  if (h->slot_gi) return VF_OK;
+  const unsigned cap = h->R.atlas_cap;
+  int rc;
+  if ((rc = dalloc(h, &h->slot_gi, cap, false))) return rc;
+  if ((rc = dalloc(h, &h->aggr, cap, false))) return rc;
+  if ((rc = dalloc(h, &h->whist, (size_t)cap * 4))) return rc;
+  if ((rc = dalloc(h, &h->staged, 4))) return rc;
+  return VF_OK;
+}
+
+// Features of every materialised brick at the current state: dev_x gets nslots x 32 fp16
+// (row s = atlas slot s). Each call also advances the 4-call water-sum history used for the
+// flux features, so call it once per tick while the proposal runs.
+int vf_fluid_proposal_features(vf_fluid* h, void* dev_x, uint64_t cap_slots, uint64_t* nslots) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = proposal_buffers(h))) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  const unsigned n = std::min(h->hctl->atlas_used, h->R.atlas_cap);
+  if (nslots) *nslots = n;
+  if (!dev_x || cap_slots < n || !n) return dev_x && cap_slots < n ? VF_ERR_INVALID : VF_OK;
+  const uint64_t nb = (uint64_t)h->R.bx * h->R.by * h->R.bz;
+  CK(cudaMemsetAsync(h->slot_gi, 0xFF, (size_t)n * 4, h->stream));
+  k_slot_map<<<(unsigned)std::min<uint64_t>((nb + 255) / 256, 8192), 256, 0, h->stream>>>(h->R, h->slot_gi, n);
+  k_slot_aggr<<<std::min(n, 16384u), 128, 0, h->stream>>>(h->R, h->slot_gi, n, h->aggr);
+  k_slot_features<<<(n + 255) / 256, 256, 0, h->stream>>>(h->R, h->aggr, n, h->whist, h->hpos, h->hctl->tick_no, (__half*)dev_x);
+  k_slot_hist<<<(n + 255) / 256, 256, 0, h->stream>>>(h->aggr, n, h->whist, h->hpos);
+  h->hpos += 1;
+  CK(cudaGetLastError());
+  return VF_OK;
+}
+
+// Labels for features taken at tick `since`: 1 where the brick woke in (since, now].
+int vf_fluid_proposal_labels(vf_fluid* h, uint32_t since_tick, float* dev_y, uint64_t nslots) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (!nslots) return VF_OK;
+  if (!dev_y) return VF_ERR_INVALID;
+  const unsigned n = (unsigned)std::min<uint64_t>(nslots, h->R.atlas_cap);
+  k_slot_labels<<<(n + 255) / 256, 256, 0, h->stream>>>(h->R, n, since_tick, h->hctl->tick_no, dev_y);
+  CK(cudaGetLastError());
+  return VF_OK;
+}
+
+// Pre-stage (L2 prefetch) the bricks whose wake probability is >= threshold; the exact FIFO still
+// decides what runs. *n_staged (optional) = bricks staged.
+int vf_fluid_stage_bricks(vf_fluid* h, const float* dev_prob, uint64_t nslots, float threshold, uint64_t* n_staged) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = proposal_buffers(h))) return rc;
+  if (!nslots) return VF_OK;
+  const unsigned n = (unsigned)std::min<uint64_t>(nslots, h->R.atlas_cap);
+  CK(cudaMemsetAsync(h->staged, 0, 4, h->stream));
+  k_stage<<<(n + 255) / 256, 256, 0, h->stream>>>(h->R, n, dev_prob, threshold, h->staged);
+  CK(cudaGetLastError());
+  if (n_staged) {
+    unsigned c = 0;
+    CK(cudaMemcpyAsync(&c, h->staged, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *n_staged = c;
+  }
   return VF_OK;
 }
 

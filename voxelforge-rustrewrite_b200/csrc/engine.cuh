@@ -93,6 +93,7 @@ struct Region {
   unsigned int* ev_chg;      // voxel-material writes
   unsigned int ev_act_cap, ev_seed_cap, ev_chg_cap;
   unsigned int* stamp;       // ncells: first event index per cell during a commit (0xFFFFFFFF idle)
+  unsigned int* last_woken;  // atlas_cap: last tick a cell of the slot's brick was drained (0 = never)
   Ctl* ctl;
 };
 

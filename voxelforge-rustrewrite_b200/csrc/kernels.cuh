@@ -2,6 +2,8 @@
 // regions, host-edit kernels (wake, displace, brush, emitters, set_partial) and inspection
 // kernels (digests, dense export, change download).
 #pragma once
+#include <cuda_fp16.h>
+
 #include "engine_dev.cuh"
 
 namespace vfe {
@@ -542,10 +544,18 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     const unsigned n = s_n;
     const bool flip = s_flip != 0;
     const unsigned long long qh = sW.qhead;
+    const unsigned tick_now = R.ctl->tick_no;
     for (unsigned i = tid; i < n; i += TICK_THREADS) {
       unsigned id = R.queue[(qh + i) & R.qmask];
       atomicAnd(&R.active[id >> 5], ~(1u << (id & 31)));
       R.cells[i] = sort_key(R, id, flip);
+      // wake history of materialised bricks (training labels of the wake proposal)
+      int x, y, z;
+      dom_xyz(R, id, x, y, z);
+      if (!outside(R, ring, x, y, z)) {
+        unsigned g = R.grid[grid_index(R, x >> 3, y >> 3, z >> 3)];
+        if (g >= 256u) R.last_woken[g - 256u] = tick_now;
+      }
     }
     __syncthreads();
     if (tid == 0) {
@@ -989,6 +999,170 @@ __global__ void k_slot_map(Region R, int* slot_brick, unsigned nslots) {
   for (unsigned long long gi = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; gi < nb; gi += (unsigned long long)gridDim.x * blockDim.x) {
     unsigned g = R.grid[gi];
     if (g >= 256u && g - 256u < nslots) slot_brick[g - 256u] = (int)gi;
+  }
+}
+
+}  // namespace vfe
+
+namespace vfe {
+
+// ------------------------------------------------------------------ wake-proposal features
+// Per materialised brick (atlas slot): aggregates of its 512 cells.
+struct SlotAggr {
+  float wsum, wmax;
+  unsigned npart, nwater, nsolid, nactive, ntop;
+  int gi;  // grid index, -1 for a slot no brick uses
+};
+
+__global__ void k_slot_aggr(Region R, const int* slot_gi, unsigned nslots, SlotAggr* out) {
+  __shared__ float s_sum[4], s_max[4];
+  __shared__ unsigned s_cnt[4][5];
+  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;  // 128 threads
+  for (unsigned s = blockIdx.x; s < nslots; s += gridDim.x) {
+    const int gi = slot_gi[s];
+    float sum = 0.f, mx = 0.f;
+    unsigned c[5] = {0, 0, 0, 0, 0};
+    if (gi >= 0) {
+      int bx = gi % R.bx, by = (gi / R.bx) % R.by, bz = gi / (R.bx * R.by);
+      if (R.ring_w) {
+        const int* rs = R.ring + 3 * ((bz / 16) * R.ring_w + (bx / 16));
+        bx = rs[0] * 16 + bx % 16;
+        bz = rs[1] * 16 + bz % 16;
+      }
+      for (unsigned l = tid; l < 512u; l += 128u) {
+        const size_t o = (size_t)s * 512u + l;
+        const unsigned m = R.amat[o];
+        const float p = R.avol[o];
+        const float v = p > 0.f ? p : (m == WATER ? 1.f : 0.f);
+        sum += v;
+        mx = fmaxf(mx, v);
+        c[0] += p > 0.f;
+        c[1] += m == WATER;
+        c[2] += (m != 0u && m != WATER);
+        const int x = bx * 8 + (int)(l & 7u), y = by * 8 + (int)((l >> 3) & 7u), z = bz * 8 + (int)(l >> 6);
+        if (in_dom(R, x, y, z)) {
+          unsigned id = dom_id(R, x, y, z);
+          c[3] += (R.active[id >> 5] >> (id & 31)) & 1u;
+        }
+        if (v > 0.f && ((l >> 3) & 7u) < 7u) {  // water with air above (within the brick)
+          const unsigned m2 = R.amat[o + 8];
+          const float p2 = R.avol[o + 8];
+          c[4] += (m2 == 0u && !(p2 > 0.f));
+        }
+      }
+    }
+    for (int off = 16; off; off >>= 1) {
+      sum += __shfl_xor_sync(FULLMASK, sum, off);
+      mx = fmaxf(mx, __shfl_xor_sync(FULLMASK, mx, off));
+      for (int k = 0; k < 5; ++k) c[k] += __shfl_xor_sync(FULLMASK, c[k], off);
+    }
+    if (lane == 0) {
+      s_sum[warp] = sum;
+      s_max[warp] = mx;
+      for (int k = 0; k < 5; ++k) s_cnt[warp][k] = c[k];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      SlotAggr a;
+      a.wsum = s_sum[0] + s_sum[1] + s_sum[2] + s_sum[3];
+      a.wmax = fmaxf(fmaxf(s_max[0], s_max[1]), fmaxf(s_max[2], s_max[3]));
+      unsigned t[5];
+      for (int k = 0; k < 5; ++k) t[k] = s_cnt[0][k] + s_cnt[1][k] + s_cnt[2][k] + s_cnt[3][k];
+      a.npart = t[0];
+      a.nwater = t[1];
+      a.nsolid = t[2];
+      a.nactive = t[3];
+      a.ntop = t[4];
+      a.gi = gi;
+      out[s] = a;
+    }
+    __syncthreads();
+  }
+}
+
+// Aggregate of the face neighbour (dx,dy,dz) of grid cell gi: its slot's, or the uniform value's.
+__device__ __forceinline__ void neighbour_aggr(const Region& R, const SlotAggr* aggr, int gi, int dx, int dy, int dz, float& wsum,
+                                               float& act, int& nslot) {
+  int bx = gi % R.bx + dx, by = (gi / R.bx) % R.by + dy, bz = gi / (R.bx * R.by) + dz;
+  wsum = 0.f;
+  act = 0.f;
+  nslot = -1;
+  if (by < 0 || by >= R.by) return;
+  if (!R.ring_w && (bx < 0 || bz < 0 || bx >= R.bx || bz >= R.bz)) return;
+  unsigned g = R.grid[grid_index(R, bx, by, bz)];
+  if (g >= 256u) {
+    nslot = (int)(g - 256u);
+    wsum = aggr[nslot].wsum;
+    act = (float)aggr[nslot].nactive;
+  } else if (g == WATER) {
+    wsum = 512.f;
+  }
+}
+
+// Features (32 fp16 per slot): water sum, max level, partial/water/solid/active counts, exposed
+// surface, the six face neighbours' water sums and active counts, water-sum changes over the last
+// four calls (own and the faces': the flux proxy), wake recency, height, bias.
+__global__ void k_slot_features(Region R, const SlotAggr* aggr, unsigned nslots, const float* hist, unsigned hpos, unsigned tick,
+                                __half* X) {
+  for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+    float f[32];
+    for (int k = 0; k < 32; ++k) f[k] = 0.f;
+    const SlotAggr a = aggr[s];
+    if (a.gi >= 0) {
+      const float old = hist[(size_t)s * 4 + ((hpos + 1) & 3u)];
+      f[0] = a.wsum / 512.f;
+      f[1] = a.wmax;
+      f[2] = a.npart / 512.f;
+      f[3] = a.nwater / 512.f;
+      f[4] = a.nsolid / 512.f;
+      f[5] = a.nactive / 512.f;
+      f[6] = a.ntop / 64.f;
+      const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+      for (int k = 0; k < 6; ++k) {
+        float w, ac;
+        int ns;
+        neighbour_aggr(R, aggr, a.gi, D[k][0], D[k][1], D[k][2], w, ac, ns);
+        f[7 + k] = w / 512.f;
+        f[13 + k] = ac / 512.f;
+        f[20 + k] = ns >= 0 ? (w - hist[(size_t)ns * 4 + ((hpos + 1) & 3u)]) / 64.f : 0.f;
+      }
+      f[19] = (a.wsum - old) / 64.f;
+      const unsigned lw = R.last_woken[s];
+      const unsigned age = lw ? tick - lw : 0xFFFFFFFFu;
+      f[26] = age <= 1u ? 1.f : 0.f;
+      f[27] = age <= 4u ? 1.f : 0.f;
+      f[28] = lw ? 1.f / (1.f + (float)age) : 0.f;
+      f[29] = (float)(((a.gi / R.bx) % R.by) * 8) / (float)R.ny;
+      f[30] = 1.f;
+      f[31] = a.nactive ? 1.f : 0.f;
+    }
+    __half2* out = reinterpret_cast<__half2*>(X + (size_t)s * 32);
+    for (int k = 0; k < 16; ++k) out[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
+  }
+}
+
+__global__ void k_slot_hist(const SlotAggr* aggr, unsigned nslots, float* hist, unsigned hpos) {
+  for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x)
+    hist[(size_t)s * 4 + (hpos & 3u)] = aggr[s].gi >= 0 ? aggr[s].wsum : 0.f;
+}
+
+// Label: a cell of the slot's brick was drained in ticks (since, now].
+__global__ void k_slot_labels(Region R, unsigned nslots, unsigned since, unsigned now, float* y) {
+  for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+    const unsigned lw = R.last_woken[s];
+    y[s] = (lw > since && lw <= now) ? 1.f : 0.f;
+  }
+}
+
+// Pre-stage the bricks the proposal expects to wake: their material and volume lines into L2.
+__global__ void k_stage(Region R, unsigned nslots, const float* prob, float thr, unsigned* staged) {
+  for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+    if (!(prob[s] >= thr)) continue;
+    const char* m = reinterpret_cast<const char*>(R.amat + (size_t)s * 512u);
+    const char* v = reinterpret_cast<const char*>(R.avol + (size_t)s * 512u);
+    for (int k = 0; k < 4; ++k) asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 128 * k));
+    for (int k = 0; k < 16; ++k) asm volatile("prefetch.global.L2 [%0];" ::"l"(v + 128 * k));
+    atomicAdd(staged, 1u);
   }
 }
 
