@@ -260,3 +260,35 @@ def test_plain_and_batched_modes_agree(vf):
     assert ra.cells == rb.cells
     for x, y in zip(a, b):
         assert x.digest() == y.digest()
+
+
+def test_download_changes_in_small_batches(vf, orc):
+    """Pending changes taken a few at a time: every changed voxel arrives exactly once."""
+    import ctypes as C
+
+    wl = vf.Workload(1)
+    w = wl.world(0)
+    sim, o = pair(vf, orc, w)
+    for box in wl.wakes(0):
+        sim.wake(*map(int, box))
+        o.wake(*map(int, box))
+    sim.tick(30)
+    o.tick(30)
+    seen = {}
+    L = vf.lib()
+    buf = (vf.Voxel * 97)()
+    while True:
+        n = C.c_uint64()
+        sim._check(L.vf_fluid_download_changes(sim.h, buf, 97, C.byref(n)), "changes")
+        got = min(n.value, 97)
+        for v in buf[:got]:
+            key = (v.x, v.y, v.z)
+            assert key not in seen
+            seen[key] = v.m
+        if n.value <= 97:
+            break
+    for (x, y, z), m in seen.items():
+        w.set_voxel(x, y, z, m)
+    om, _ = o.export_box(0, 0, 0, 64, 64, 64)
+    hm = np.array([[[w.get_voxel(x, y, z) for x in range(64)] for y in range(64)] for z in range(64)], np.uint8)
+    assert np.array_equal(hm, om)

@@ -455,13 +455,17 @@ int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t
   if (n) *n = total;
   uint64_t take = std::min(total, cap);
   if (!take || !out) return VF_OK;
-  if ((rc = ensure_scratch(h, take * sizeof(Voxel)))) return rc;
+  const size_t vox_bytes = align16(take * sizeof(Voxel));
+  if ((rc = ensure_scratch(h, vox_bytes + (total - take) * 4))) return rc;
   k_gather_changes<<<(unsigned)std::min<uint64_t>((take + 255) / 256, 4096), 256, 0, h->stream>>>(h->R, take, (Voxel*)h->scratch);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->scratch, take * sizeof(Voxel), cudaMemcpyDeviceToHost, h->stream));
   if (take < total) {
-    // keep the rest pending: move it to the front of the list
-    CK(cudaMemcpyAsync(h->R.chg, h->R.chg + take, (total - take) * 4, cudaMemcpyDeviceToDevice, h->stream));
+    // keep the rest pending: move it to the front of the list through the scratch buffer (the
+    // source and destination ranges may overlap)
+    unsigned* tmp = (unsigned*)((char*)h->scratch + vox_bytes);
+    CK(cudaMemcpyAsync(tmp, h->R.chg + take, (total - take) * 4, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->R.chg, tmp, (total - take) * 4, cudaMemcpyDeviceToDevice, h->stream));
   }
   unsigned long long left = total - take;
   CK(cudaMemcpyAsync(&h->R.ctl->nchg, &left, 8, cudaMemcpyHostToDevice, h->stream));
