@@ -124,6 +124,20 @@ int vf_fluid_update(vf_fluid* h, float dt, int32_t* changed);
  * Writes at most cap entries, sets *n to the total pending; entries not copied stay pending. */
 int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n);
 
+/* The same download for callers that must not allocate device memory while they run (no
+ * counterpart in the reference, whose fluid lives in host memory). A per-frame game loop cannot
+ * take the device-wide stall an allocation may cause, and an engine that fixes every subsystem's
+ * memory budget at start-up forbids allocating later; this entry point calls no cudaMalloc,
+ * cudaFree or allocating library routine. It gathers through one fixed device array of
+ * VF_NOALLOC_MAX_CHANGES changes that each device keeps until the process exits; cap above that
+ * is rejected with VF_ERR_RANGE. The first call on a device looks the array's address up (make
+ * that first call before any stream capture). Every call on a device shares the array and
+ * overwrites what the last call left there, so calls whose GPU work overlaps race: serialise them.
+ * Same contract as vf_fluid_download_changes otherwise: at most cap entries, *n = total pending,
+ * the rest stay pending. */
+#define VF_NOALLOC_MAX_CHANGES 65536
+int vf_fluid_download_changes_noalloc(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n);
+
 /* FluidSim::volume (src/fluid.rs:251-260). */
 int vf_fluid_volume(vf_fluid* h, int32_t x, int32_t y, int32_t z, float* out);
 /* FluidSim::idle (:265-267). */

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <string>
 #include <tuple>
+#include <mutex>
 #include <vector>
 
 #include "../../include/vf_fluid.h"
@@ -469,6 +470,81 @@ int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t
   }
   unsigned long long left = total - take;
   CK(cudaMemcpyAsync(&h->R.ctl->nchg, &left, 8, cudaMemcpyHostToDevice, h->stream));
+  return sync_ctl(h);
+}
+
+// ------------------------------------------------------- allocation-free change download
+// Some callers must not allocate device memory while they run: a game's per-frame loop cannot
+// afford the device-wide stall that cudaMalloc/cudaFree may cause, and an engine that hands a
+// fixed memory budget to its subsystems at start-up forbids allocations after that. For them,
+// vf_fluid_download_changes_noalloc gathers into this fixed array instead of the handle's
+// growable scratch buffer. The array is VF_NOALLOC_MAX_CHANGES entries (1 MiB) on every device
+// that loads the library, held until the process exits, and shared by every call on that device:
+// each call overwrites what the previous one left there, so calls whose work overlaps on the GPU
+// (for example from two host threads or two streams at once) race and must be serialised.
+static __device__ __align__(256) Voxel g_noalloc_changes[VF_NOALLOC_MAX_CHANGES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+Voxel* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// The device address of the array, looked up once per device with that device current.
+int noalloc_buffer(vf_fluid* h, Voxel** out) {
+  if (h->device < 0 || h->device >= NOALLOC_MAX_DEVICES) return fail(h, VF_ERR_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[h->device]) {
+    CK(cudaSetDevice(h->device));
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_changes);
+    if (e != cudaSuccess || !p) return fail(h, VF_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[h->device] = (Voxel*)p;
+  }
+  *out = g_noalloc_ptr[h->device];
+  return VF_OK;
+}
+}  // namespace
+
+// Takes the last `take` pending changes (the list's order carries no meaning), writes their final
+// material into `out`, clears their pending bits and shortens the list, so nothing needs moving.
+__global__ void k_gather_changes_tail(Region R, unsigned long long total, unsigned long long take, Voxel* out) {
+  const unsigned long long first = total - take;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < take; i += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned id = R.chg[first + i];
+    int x, y, z;
+    dom_xyz(R, id, x, y, z);
+    CD c = load_cell(R, R.ring, x, y, z);
+    Voxel v;
+    v.x = x;
+    v.y = y;
+    v.z = z;
+    v.m = c.mat;
+    v.pad[0] = v.pad[1] = v.pad[2] = 0;
+    out[i] = v;
+    atomicAnd(&R.chgbits[id >> 5], ~(1u << (id & 31)));
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) R.ctl->nchg = first;
+}
+
+int vf_fluid_download_changes_noalloc(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (cap > VF_NOALLOC_MAX_CHANGES) {
+    char b[160];
+    snprintf(b, sizeof b, "download_changes_noalloc: cap %llu exceeds its fixed buffer of %d changes per call",
+             (unsigned long long)cap, VF_NOALLOC_MAX_CHANGES);
+    return fail(h, VF_ERR_RANGE, b);
+  }
+  Voxel* buf = nullptr;
+  if ((rc = noalloc_buffer(h, &buf))) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  const uint64_t total = std::min<uint64_t>(h->hctl->nchg, h->R.chg_cap);
+  if (n) *n = total;
+  const uint64_t take = std::min(total, cap);
+  if (!take || !out) return VF_OK;
+  k_gather_changes_tail<<<(unsigned)std::min<uint64_t>((take + 255) / 256, 256), 256, 0, h->stream>>>(h->R, total, take, buf);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, buf, take * sizeof(Voxel), cudaMemcpyDeviceToHost, h->stream));
   return sync_ctl(h);
 }
 
