@@ -23,6 +23,18 @@ NFEAT = 32
 HORIZON = 8
 
 
+def _current_stream() -> int:
+    import torch
+
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _sim_stream(sim, torch):
+    """A torch stream context on the sim's own stream, so tensors made for the sim's kernels are
+    ordered with them."""
+    return torch.cuda.stream(torch.cuda.ExternalStream(sim.stream()))
+
+
 def _sig():
     L = lib()
     P = C.c_void_p
@@ -72,15 +84,18 @@ class MLP:
         p = np.ascontiguousarray(p, np.float32)
         lib().vf_mlp_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)))
 
-    def forward(self, x, torch, stream=0):
-        """x: (n, 32) float16 CUDA tensor -> (n,) float32 probabilities."""
+    def forward(self, x, torch, stream=None):
+        """x: (n, 32) float16 CUDA tensor -> (n,) float32 probabilities (on torch's current stream
+        unless a stream handle is given)."""
+        stream = _current_stream() if stream is None else stream
         out = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
         rc = lib().vf_mlp_forward(self.h, C.c_void_p(x.data_ptr()), x.shape[0], C.c_void_p(out.data_ptr()), C.c_void_p(stream))
         if rc:
             raise VfError(rc, "vf_mlp_forward")
         return out
 
-    def grads(self, x, y, stream=0) -> np.ndarray:
+    def grads(self, x, y, stream=None) -> np.ndarray:
+        stream = _current_stream() if stream is None else stream
         g = np.zeros(self.nparams, np.float32)
         rc = lib().vf_mlp_grads(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), x.shape[0], g.ctypes.data_as(C.POINTER(C.c_float)),
                                 C.c_void_p(stream))
@@ -88,7 +103,8 @@ class MLP:
             raise VfError(rc, "vf_mlp_grads")
         return g
 
-    def train_step(self, x, y, lr: float, stream=0, want_loss=False):
+    def train_step(self, x, y, lr: float, stream=None, want_loss=False):
+        stream = _current_stream() if stream is None else stream
         loss = C.c_float(0.0)
         rc = lib().vf_mlp_train_step(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), x.shape[0], lr,
                                      C.byref(loss) if want_loss else None, C.c_void_p(stream))
@@ -134,23 +150,34 @@ def features(sim, torch):
     rc = L.vf_fluid_proposal_features(sim.h, None, 0, C.byref(n))
     if rc:
         raise VfError(rc, "proposal_features")
-    x = torch.zeros((max(n.value, 1), NFEAT), dtype=torch.float16, device="cuda")
+    with _sim_stream(sim, torch):
+        x = torch.zeros((max(n.value, 1), NFEAT), dtype=torch.float16, device="cuda")
     rc = L.vf_fluid_proposal_features(sim.h, C.c_void_p(x.data_ptr()), x.shape[0], C.byref(n))
     if rc:
         raise VfError(rc, "proposal_features")
+    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream()))
+    x.record_stream(torch.cuda.current_stream())
     return x[: n.value], n.value
 
 
 def labels(sim, since_tick: int, nslots: int, torch):
     L = _sig()
-    y = torch.zeros(max(nslots, 1), dtype=torch.float32, device="cuda")
+    with _sim_stream(sim, torch):
+        y = torch.zeros(max(nslots, 1), dtype=torch.float32, device="cuda")
     rc = L.vf_fluid_proposal_labels(sim.h, since_tick, C.c_void_p(y.data_ptr()), nslots)
     if rc:
         raise VfError(rc, "proposal_labels")
+    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream()))
+    y.record_stream(torch.cuda.current_stream())
     return y[:nslots]
 
 
 def stage(sim, prob, threshold: float = 0.5) -> int:
+    """Pre-stage the bricks whose probability reaches the threshold (prob made on torch's current
+    stream; the sim's stream waits for it)."""
+    import torch
+
+    torch.cuda.ExternalStream(sim.stream()).wait_stream(torch.cuda.current_stream())
     L = _sig()
     n = C.c_uint64()
     rc = L.vf_fluid_stage_bricks(sim.h, C.c_void_p(prob.data_ptr()), prob.shape[0], threshold, C.byref(n))
@@ -207,7 +234,9 @@ def train(mlp: MLP, X, Y, torch, epochs: int = 4, batch: int = 8192, lr: float =
         for i in range(0, n, batch):
             idx = perm[i : i + batch]
             xb, yb = X[idx].contiguous(), Y[idx].contiguous()
-            losses.append(mlp.train_step(xb, yb, lr, want_loss=(i == 0)))
+            loss = mlp.train_step(xb, yb, lr, want_loss=(i == 0))
+            if i == 0:
+                losses.append(loss)  # loss of each epoch's first batch, before its step
     return losses
 
 
@@ -226,3 +255,31 @@ def score(pred, Y) -> Score:
     tp = int((p & t).sum())
     npos, npred = int(t.sum()), int(p.sum())
     return Score(tp / npos if npos else 1.0, tp / npred if npred else 1.0, npos, npred, int(Y.numel()))
+
+
+# Trace runs the default network trains on: (workload id, scale, seed, warm ticks, ticks, regions)
+# - the basin, the dam break (x/z scaled to 1/4) and eight small batched regions.
+DEFAULT_TRACES = [(1, 1.0, 1, 10, 60, 1), (2, 0.25, 3, 5, 40, 1), (3, 0.08, 2, 5, 40, 8)]
+
+
+def train_default(vf, torch, seed: int = 5, traces=None, epochs: int = 8):
+    """Collect traces of the exact engine, train a fresh network on 80% of them on the GPU and
+    score it on the other 20% against the persistence rule. Returns (mlp, dict of results)."""
+    import time
+
+    t0 = time.perf_counter()
+    X, Y, B = collect(vf, torch, traces or DEFAULT_TRACES, every=2)
+    t1 = time.perf_counter()
+    n = X.shape[0]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    perm = torch.randperm(n, device="cuda", generator=g)
+    tr, te = perm[: int(0.8 * n)], perm[int(0.8 * n):]
+    mlp = MLP(seed=seed)
+    losses = train(mlp, X[tr].contiguous(), Y[tr].contiguous(), torch, epochs=epochs, batch=4096, lr=2e-3)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    s = score(mlp.forward(X[te].contiguous(), torch), Y[te])
+    base = score(B[te], Y[te])
+    return mlp, {"samples": n, "collect_s": t1 - t0, "train_s": t2 - t1, "loss_first": losses[0], "loss_last": losses[-1],
+                 "heldout": s.__dict__, "persistence": base.__dict__}
