@@ -13,6 +13,14 @@ namespace vfe {
 
 constexpr unsigned FULLMASK = 0xFFFFFFFFu;
 
+// Per-call cycle counters inside a cell (pressure search, writes, activation log) cost issue
+// slots on the sweep's critical path; they are compiled in only with VF_FINE_PROFILE.
+#ifdef VF_FINE_PROFILE
+__device__ __forceinline__ long long fine_clock() { return clock64(); }
+#else
+__device__ __forceinline__ long long fine_clock() { return 0; }
+#endif
+
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -85,56 +93,62 @@ struct WS {
   // parallel at the tick's end (deferred); host edits apply them at once.
   bool deferred;
   unsigned nact, nseed, nchg;  // event-log cursors (deferred mode)
-  // store-forwarding table of the prefetching sweep (null outside it)
-  unsigned* fwd_key;           // [2][FWD_CAP]
-  unsigned* fwd_val;           // [2][FWD_CAP] material
-  float* fwd_part;             // [2][FWD_CAP]
-  int ft;                      // current table (epoch parity)
+  // store-forwarding table of the prefetching sweep (null outside it) and the sequence number
+  // (sorted index + 1) of the cell the sweep is processing
+  struct FwdEntry* fwd;
+  unsigned seq;
   unsigned long long t_wait, t_pull, t_act, t_write, t_top, t_pc, t_tail;  // cycle counters (profiling)
 };
 
-constexpr int FWD_CAP = 1024;  // forwarding entries per epoch table
+// Store forwarding for the prefetching sweep: a direct-mapped table of the sweep's latest writes.
+// An entry holds the cell id (tag), the writer's sequence number (sorted index + 1) and the
+// written material, partial volume and atlas slot. A prefetched footprint cell fetched when
+// `c0` cells were finished is current unless its entry's sequence is above c0; then the entry
+// supplies the value if its tag is the cell, and otherwise (another cell wrote over the entry)
+// the sweep re-reads the cell from memory, which holds every write of the sweep.
+constexpr unsigned FWD_SIZE = 4096;
+struct __align__(16) FwdEntry {
+  unsigned tag;   // cell id
+  unsigned meta;  // writer sequence (low 16 bits) | material << 16
+  float part;
+  unsigned slot;
+};
+static_assert(MAX_CELLS_PER_TICK < 65536u, "writer sequence numbers must fit 16 bits");
+
+// Index of a cell in the table: low bits of x, z and y, so that the cells written by the last
+// few dozen cells of the sweep (one neighbourhood of rows and layers) rarely share an entry.
+__device__ __forceinline__ unsigned fwd_index(int x, int y, int z) {
+  return ((unsigned)x & 127u) | (((unsigned)z & 7u) << 7) | (((unsigned)y & 3u) << 10);
+}
+
+__device__ __forceinline__ void fwd_insert(WS& W, unsigned id, int x, int y, int z, const CD& c) {
+  FwdEntry e;
+  e.tag = id;
+  e.meta = W.seq | ((unsigned)c.mat << 16);
+  e.part = c.part;
+  e.slot = c.slot;
+  W.fwd[fwd_index(x, y, z)] = e;
+}
+
+// Patch a prefetched cell (fetched when c0 cells were finished). Returns false when the value
+// cannot be told from the table and must be re-read from memory.
+__device__ __forceinline__ bool fwd_patch(const FwdEntry* tab, unsigned id, int x, int y, int z, unsigned c0, CD& c) {
+  const FwdEntry e = tab[fwd_index(x, y, z)];
+  if ((e.meta & 0xFFFFu) <= c0) return true;  // not written since the fetch
+  if (e.tag != id) return false;
+  c.mat = (unsigned char)(e.meta >> 16);
+  c.part = e.part;
+  c.slot = e.slot;
+  return true;
+}
+
 constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
-
-__device__ __forceinline__ unsigned fwd_hash(unsigned id) { return (id * 2654435761u) >> 22; }  // 10 bits
-
-// Record (id -> mat, part) as the latest value this sweep wrote (lane-local call).
-__device__ __forceinline__ void fwd_insert(WS& W, unsigned id, unsigned char mat, float part) {
-  unsigned* keys = W.fwd_key + W.ft * FWD_CAP;
-  unsigned h = fwd_hash(id);
-  for (int k = 0; k < FWD_CAP; ++k) {
-    unsigned cur = keys[h];
-    if (cur == id) break;
-    if (cur == EMPTY_ID) {
-      unsigned old = atomicCAS(&keys[h], EMPTY_ID, id);
-      if (old == EMPTY_ID || old == id) break;
-    }
-    h = (h + 1) & (FWD_CAP - 1);
-  }
-  W.fwd_val[W.ft * FWD_CAP + h] = mat;
-  W.fwd_part[W.ft * FWD_CAP + h] = part;
-}
-
-__device__ __forceinline__ bool fwd_lookup_t(const WS& W, int t, unsigned id, unsigned char& mat, float& part) {
-  const unsigned* keys = W.fwd_key + t * FWD_CAP;
-  unsigned h = fwd_hash(id);
-  for (int k = 0; k < FWD_CAP; ++k) {
-    unsigned cur = keys[h];
-    if (cur == id) {
-      mat = (unsigned char)W.fwd_val[t * FWD_CAP + h];
-      part = W.fwd_part[t * FWD_CAP + h];
-      return true;
-    }
-    if (cur == EMPTY_ID) return false;
-    h = (h + 1) & (FWD_CAP - 1);
-  }
-  return false;
-}
 
 struct Smem {
   unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
   unsigned* pq;             // PRESS_QCAP
   const int* ring;
+  float* pv;                // PRESS_QCAP: volume of each queued cell when it was queued
 };
 
 __device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
@@ -231,39 +245,35 @@ __device__ __forceinline__ bool set_volume_needs_slot(const CD& c, float vol) {
 }
 
 // FluidSim::set_volume (fluid.rs:327-355) on one lane's cell; c.slot must be valid when
-// set_volume_needs_slot said so. Returns "the voxel changed".
-__device__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, unsigned id, float vol, long long& pdelta, bool deferred = false) {
+// set_volume_needs_slot said so. Returns "the voxel changed". Written as selects: the snapping
+// (<= 1e-6 -> 0, >= 1-1e-4 -> full), the partial entry and the show/hide hysteresis each decide a
+// value, and the stores are predicated.
+__device__ __forceinline__ bool set_volume_lane(const Region& R, CD& c, int x, int y, int z, unsigned id, float vol, long long& pdelta,
+                                                bool deferred = false) {
   const unsigned l = local_index(x, y, z);
   const bool is_water = c.mat == WATER;
-  if (vol <= 1e-6f) {
-    erase_part(R, c, l, pdelta);
-    if (is_water) {
-      write_mat(R, c, l, id, 0, deferred);
-      return true;
-    }
-    return false;
-  }
-  if (vol >= full_level()) {
-    erase_part(R, c, l, pdelta);
-    if (!is_water) {
-      write_mat(R, c, l, id, WATER, deferred);
-      return true;
-    }
-    return false;
-  }
-  if (c.slot == NOSLOT) return false;
-  if (!(c.part > 0.0f)) pdelta += 1;
-  R.avol[(size_t)c.slot * 512u + l] = vol;
-  c.part = vol;
-  if (is_water && vol < HIDE_BELOW) {
-    write_mat(R, c, l, id, 0, deferred);
-    return true;
-  }
-  if (!is_water && vol >= SHOW_AT) {
-    write_mat(R, c, l, id, WATER, deferred);
-    return true;
-  }
-  return false;
+  const bool has = c.slot != NOSLOT;  // false only when materialisation failed (status set)
+  const bool low = vol <= 1e-6f;
+  const bool high = !low && vol >= full_level();
+  const bool mid = !low && !high;
+  const bool had = has && c.part > 0.0f;
+  const float npart = mid ? vol : 0.0f;
+  const unsigned char nmat = low ? (unsigned char)0
+                           : high ? (unsigned char)WATER
+                           : (is_water && vol < HIDE_BELOW) ? (unsigned char)0
+                           : (!is_water && vol >= SHOW_AT) ? (unsigned char)WATER
+                           : c.mat;
+  const bool wpart = has && (mid || had);
+  const bool wmat = has && nmat != c.mat;
+  const bool ch = mid ? wmat : nmat != c.mat;
+  pdelta += (mid && has && !had) ? 1 : 0;
+  pdelta -= (!mid && had) ? 1 : 0;
+  if (wpart) R.avol[(size_t)c.slot * 512u + l] = npart;
+  if (wmat) R.amat[(size_t)c.slot * 512u + l] = nmat;
+  if (has) c.part = npart;
+  if (wmat) c.mat = nmat;
+  if (wmat && !deferred) record_change(R, id);
+  return ch;
 }
 
 // Append per-lane events (lane order) to a log; returns the new cursor.
@@ -280,18 +290,18 @@ __device__ __forceinline__ unsigned log_append(const Region& R, unsigned* log, u
 // Warp: lanes with `w` write `vol` into their cell through set_volume. Returns whether any
 // voxel changed.
 __device__ bool warp_set_volume(const Region& R, WS& W, bool w, CD& c, int x, int y, int z, float vol) {
-  const long long t0 = clock64();
+  const long long t0 = fine_clock();
   bool need = w && set_volume_needs_slot(c, vol);
   if (__any_sync(FULLMASK, need)) materialize_lanes(R, need, c.gi, c.slot);
   bool ch = false;
   const unsigned id = (w && in_dom(R, x, y, z)) ? dom_id(R, x, y, z) : 0u;
   if (w) {
     ch = set_volume_lane(R, c, x, y, z, id, vol, W.pdelta, W.deferred);
-    if (W.fwd_key) fwd_insert(W, id, c.mat, c.part);
+    if (W.fwd) fwd_insert(W, id, x, y, z, c);
   }
   if (W.deferred) W.nchg = log_append(R, R.ev_chg, R.ev_chg_cap, W.nchg, ch, id, 9);
   __syncwarp();
-  W.t_write += clock64() - t0;
+  W.t_write += fine_clock() - t0;
   return __any_sync(FULLMASK, ch);
 }
 
@@ -307,6 +317,7 @@ struct ActList {
   unsigned mask;
   __device__ __forceinline__ void reset(int x, int y, int z) {
     cx = x; cy = y; cz = z; mask = 0;
+    sx = sy = sz = 0;
   }
   __device__ __forceinline__ void source(int a, int b, int c) {
     sx = a; sy = b; sz = c; mask |= 1u;
@@ -314,14 +325,11 @@ struct ActList {
   __device__ __forceinline__ void slot(int g) { mask |= 1u << g; }
   // slot g's centre and kind (1 or 7)
   __device__ __forceinline__ int get(int g, int& x, int& y, int& z) const {
-    if (g == 0) {
-      x = sx; y = sy; z = sz;
-      return 1;
-    }
-    x = cx + (g == 3) - (g == 4);
-    y = cy - (g == 2);
-    z = cz + (g == 5) - (g == 6);
-    return 7;
+    const bool src = g == 0;
+    x = src ? sx : cx + (g == 3) - (g == 4);
+    y = src ? sy : cy - (g == 2);
+    z = src ? sz : cz + (g == 5) - (g == 6);
+    return src ? 1 : 7;
   }
 };
 
@@ -363,7 +371,7 @@ constexpr unsigned ACT_AROUND = 0x80000000u;
 
 __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
   if (A.mask == 0) return;
-  const long long t0 = clock64();
+  const long long t0 = fine_clock();
   const unsigned lane = lane_id();
   if (W.deferred) {  // one log word per call, in program order (expanded by the commit)
     bool v = lane < 8 && ((A.mask >> lane) & 1u);
@@ -380,7 +388,7 @@ __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
     }
     W.nact = log_append(R, R.ev_act, R.ev_act_cap, W.nact, v, word, 10);
     __syncwarp();
-    W.t_act += clock64() - t0;
+    W.t_act += fine_clock() - t0;
     return;
   }
   // immediate mode: expand the slots into single cells, 32 per round
@@ -412,7 +420,7 @@ __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
     activate_round(R, W, valid, x, y, z);
   }
   if (W.qtail - W.qhead > R.qmask + 1ull) set_status(R, ST_OOM, 4);
-  W.t_act += clock64() - t0;
+  W.t_act += fine_clock() - t0;
 }
 
 // FluidSim::seed_level (fluid.rs:312-316); warp-uniform call.
@@ -461,14 +469,25 @@ __device__ __forceinline__ void dir5(int d, int& dx, int& dy, int& dz) {
   dz = (d == 3) - (d == 4);
 }
 
+// Queue entries a pressure search examines per round: lane 5j+d loads neighbour d of entry j.
+constexpr unsigned PB = 6;
+
 // FluidSim::pressure_pull (fluid.rs:511-561), warp-cooperative. fp[2..6] = up,+x,-x,+z,-z.
 // Appends the source's activation to A and seeds it. Returns the volume taken.
+//
+// The search examines PB queue entries per round (their 5 neighbours in one load round) and
+// keeps the reference's queue order exactly: the search writes nothing until it ends, so an
+// entry's volume is the one seen when it was queued; the first entry (in queue order) that is a
+// surface cell above the start wins, and entries after it in the round are dropped; otherwise
+// the round's expansions are appended in entry-major, direction order, with the side-step
+// budget counted in that order and duplicates inside the round left to their first occurrence.
 __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int x, int y, int z, float need, const CD* fp) {
   const unsigned lane = lane_id();
   const float FULL = full_level();
-  // start cells: full up/side neighbours (fluid.rs:518-525); none -> the BFS examines nothing
+  // start cells: full up/side neighbours (fluid.rs:518-525); none -> the search examines nothing
   bool ok = false;
   unsigned nid = 0;
+  float nvol = 0.0f;
   if (lane < 5) {
     int dx, dy, dz;
     dir5((int)lane, dx, dy, dz);
@@ -476,7 +495,10 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     // constant-index selects keep fp in registers (a lane-dependent index would spill it)
     const CD cd = lane == 0 ? fp[2] : lane == 1 ? fp[3] : lane == 2 ? fp[4] : lane == 3 ? fp[5] : fp[6];
     ok = a >= 0 && c >= 0 && !cd_solid(cd) && cd_volume(cd) >= FULL;
-    if (ok) nid = dom_id(R, a, b, c);
+    if (ok) {
+      nid = dom_id(R, a, b, c);
+      nvol = cd_volume(cd);
+    }
   }
   unsigned bm = __ballot_sync(FULLMASK, ok);
   unsigned qlen = (unsigned)__popc(bm);
@@ -490,59 +512,70 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
   if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
   __syncwarp();
   if (ok) {
-    S.pq[__popc(bm & lanemask_lt())] = nid;
+    const unsigned pos = (unsigned)__popc(bm & lanemask_lt());
+    S.pq[pos] = nid;
+    S.pv[pos] = nvol;
     vis_insert(S.vis, nid, W.epoch);
   }
   __syncwarp();
+  const unsigned j = lane / 5u, d = lane - 5u * (lane / 5u);
   unsigned side = 0, i = 0;
   float got = 0.0f;
   while (i < qlen && i < PRESSURE_SEARCH) {
-    unsigned e = S.pq[i];
-    ++i;
-    int a, b, c;
-    dom_xyz(R, e, a, b, c);
-    int na = a, nb = b, nc = c;
-    if (lane >= 1 && lane <= 5) {
+    const unsigned k = min(PB, min(qlen - i, PRESSURE_SEARCH - i));
+    const bool act = j < k;
+    int a = 0, b = 0, c = 0, na = 0, nb = 0, nc = 0;
+    float here = 0.0f;
+    CD cd = CD{0.0f, NOSLOT, 0u, 0, true};
+    if (act) {
+      const unsigned e = S.pq[i + j];
+      here = S.pv[i + j];
+      dom_xyz(R, e, a, b, c);
       int dx, dy, dz;
-      dir5((int)lane - 1, dx, dy, dz);
-      na += dx;
-      nb += dy;
-      nc += dz;
+      dir5((int)d, dx, dy, dz);
+      na = a + dx;
+      nb = b + dy;
+      nc = c + dz;
+      cd = load_cell(R, S.ring, na, nb, nc);
     }
-    CD cd;
-    if (lane < 6) cd = load_cell(R, S.ring, na, nb, nc);
-    else cd = CD{0.0f, NOSLOT, 0u, 0, true};
-    float here = __shfl_sync(FULLMASK, cd_volume(cd), 0);
-    bool top_l = (lane == 1) && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f);
-    bool top = __shfl_sync(FULLMASK, top_l, 1);
-    if (top && b > y && here > 0.0f) {
-      float take = fminf(need, here);
-      float nv = __fsub_rn(here, take);
-      CD c0 = shfl_cd(cd, 0);
-      W.changed |= warp_set_volume(R, W, lane == 0, c0, a, b, c, nv);
-      A.source(a, b, c);
-      seed_level(R, W, a, b, c);
+    // surface test of each entry on its up neighbour (fluid.rs:534-535)
+    const bool win = act && d == 0u && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f) && b > y && here > 0.0f;
+    const unsigned wm = __ballot_sync(FULLMASK, win);
+    if (wm) {
+      const int wl = __ffs(wm) - 1;
+      const int wa = __shfl_sync(FULLMASK, a, wl), wb = __shfl_sync(FULLMASK, b, wl), wc = __shfl_sync(FULLMASK, c, wl);
+      const float wh = __shfl_sync(FULLMASK, here, wl);
+      const float take = fminf(need, wh);
+      const float nv = __fsub_rn(wh, take);
+      CD c0 = CD{0.0f, NOSLOT, 0u, 0, true};
+      if (lane == 0) c0 = load_cell(R, S.ring, wa, wb, wc);
+      W.changed |= warp_set_volume(R, W, lane == 0, c0, wa, wb, wc, nv);
+      A.source(wa, wb, wc);
+      seed_level(R, W, wa, wb, wc);
       got = take;
+      i += (unsigned)wl / 5u + 1u;
       break;
     }
-    bool cand = false;
-    if (lane >= 1 && lane <= 5) cand = !(na < 0 || nc < 0 || nb >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f);
-    bool sc = cand && lane >= 2 && nb == y;
-    unsigned sm = __ballot_sync(FULLMASK, sc);
+    // expansions (fluid.rs:541-556)
+    bool cand = act && !(na < 0 || nc < 0 || nb >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f);
+    const bool sc = cand && d >= 1u && nb == y;
+    const unsigned sm = __ballot_sync(FULLMASK, sc);
     if (sc && side + (unsigned)__popc(sm & lanemask_lt()) + 1u > 24u) cand = false;
     side += (unsigned)__popc(sm);
+    const unsigned id = cand ? dom_id(R, na, nb, nc) : (0xFFFFFFFFu - lane);
+    const unsigned peers = __match_any_sync(FULLMASK, id);
     bool isnew = false;
-    unsigned id = 0;
-    if (cand) {
-      id = dom_id(R, na, nb, nc);
-      isnew = vis_insert(S.vis, id, W.epoch);
-    }
-    unsigned nm = __ballot_sync(FULLMASK, isnew);
+    if (cand && !(peers & lanemask_lt())) isnew = vis_insert(S.vis, id, W.epoch);
+    const unsigned nm = __ballot_sync(FULLMASK, isnew);
     if (isnew) {
-      unsigned pos = qlen + (unsigned)__popc(nm & lanemask_lt());
-      if (pos < PRESS_QCAP) S.pq[pos] = id;
+      const unsigned pos = qlen + (unsigned)__popc(nm & lanemask_lt());
+      if (pos < PRESS_QCAP) {
+        S.pq[pos] = id;
+        S.pv[pos] = cd_volume(cd);
+      }
     }
     qlen += (unsigned)__popc(nm);
+    i += k;
     __syncwarp();
   }
   W.bfs_visits += i;
@@ -588,9 +621,9 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   const float v0 = vol;
   // 0. pressure (fluid.rs:594-601)
   if (vol < FULL && W.pulls < MAX_PULLS_PER_TICK) {
-    const long long tp = clock64();
+    const long long tp = fine_clock();
     float got = pressure_pull(R, W, S, A, x, y, z, __fsub_rn(1.0f, vol), fp);
-    W.t_pull += clock64() - tp;
+    W.t_pull += fine_clock() - tp;
     W.pulls += 1;
     W.pull_attempts += 1;
     if (got > 0.0f) {

@@ -135,14 +135,14 @@ struct TickSmem {
   unsigned hist[TICK_WARPS * 256];
   unsigned sred[2 * 256 + 64];
   unsigned pq[PRESS_QCAP];
+  float pv[PRESS_QCAP];
   unsigned long long vis[VIS_CAP];
   int ring[3 * 16 * 16];
   CD pf[PF_RING][7];            // prefetched footprints (self, below, up, +x, -x, +z, -z)
   unsigned pf_ready[PF_RING];   // the cell index whose footprint a slot holds
   int pxyz[PF_RING][4];         // the cell's coordinates and domain id
-  unsigned fwd_key[2 * FWD_CAP];
-  unsigned fwd_val[2 * FWD_CAP];
-  float fwd_part[2 * FWD_CAP];
+  unsigned pf_c0[PF_RING];      // cells the sweep had finished when the slot's footprint was fetched
+  FwdEntry fwd[FWD_SIZE];       // the sweep's latest writes (store forwarding)
   unsigned consumed;            // cells the sweep has finished
   unsigned abort;               // a wait gave up: every warp leaves the sweep
   unsigned scan[TICK_WARPS + 1];
@@ -166,10 +166,8 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.changed = false;
   W.deferred = false;
   W.nact = W.nseed = W.nchg = 0;
-  W.fwd_key = nullptr;
-  W.fwd_val = nullptr;
-  W.fwd_part = nullptr;
-  W.ft = 0;
+  W.fwd = nullptr;
+  W.seq = 0;
   W.t_wait = W.t_pull = W.t_act = W.t_write = W.t_top = W.t_pc = W.t_tail = 0;
 }
 
@@ -355,8 +353,9 @@ __device__ void commit_chgs(const Region& R, unsigned n) {
 
 // ------------------------------------------------------------------------ the sweep
 // Warp 0 walks the sorted cells (the reference's order); warps 1.. prefetch footprints of the
-// cells ahead into a shared-memory ring. Values the sweep wrote after a footprint was fetched
-// are taken from a forwarding table that holds every write of the last 64..128 cells.
+// cells ahead into a shared-memory ring, each stamped with the number of cells the sweep had
+// finished when it was fetched. Values the sweep wrote after a fetch come from the
+// store-forwarding table (or, when the table cannot tell, from memory).
 __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   if (tid == 0) {
@@ -364,72 +363,49 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     sm.abort = 0;
   }
   for (unsigned i = tid; i < PF_RING; i += TICK_THREADS) sm.pf_ready[i] = 0xFFFFFFFFu;
-  for (unsigned i = tid; i < 2 * FWD_CAP; i += TICK_THREADS) sm.fwd_key[i] = EMPTY_ID;
+  for (unsigned i = tid; i < FWD_SIZE; i += TICK_THREADS) sm.fwd[i].meta = 0u;
   __syncthreads();
   if (warp == 0) {
     WS W = sW;
-    W.fwd_key = sm.fwd_key;
-    W.fwd_val = sm.fwd_val;
-    W.fwd_part = sm.fwd_part;
-    W.ft = 0;
-    Smem S{sm.vis, sm.pq, ring};
+    W.fwd = sm.fwd;
+    Smem S{sm.vis, sm.pq, ring, sm.pv};
+    const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
+    // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
+    const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
+    const unsigned oid = (unsigned)ox + (unsigned)oy * (unsigned)R.PX + (unsigned)oz * pxy;
     for (unsigned r = 0; r < n; ++r) {
-      if (r && (r & 63u) == 0u) {  // new epoch: the table of two epochs ago is reused
-        W.ft ^= 1;
-        for (int i = lane; i < FWD_CAP; i += 32) sm.fwd_key[W.ft * FWD_CAP + i] = EMPTY_ID;
-        __syncwarp();
-      }
       const unsigned slot = r % PF_RING;
-      // wait (lane 0, bounded) for the footprint of cell r, then share the outcome
-      unsigned ok = 1u;
+      // wait (bounded) for the footprint of cell r; every lane reads the same word
       const long long tw = clock64();
-      if (lane == 0) {
-        unsigned long long spins = 0;
-        while (*(volatile unsigned*)&sm.pf_ready[slot] != r) {
-          if (++spins > SPIN_CAP_SLEEP) {
-            ok = 0u;
-            break;
-          }
-          __nanosleep(20);
-        }
-        __threadfence_block();
+      unsigned long long spins = 0;
+      while (*(volatile unsigned*)&sm.pf_ready[slot] != r) {
+        if (++spins > SPIN_CAP_SLEEP) break;
+        __nanosleep(20);
       }
-      ok = __shfl_sync(FULLMASK, ok, 0);
-      W.t_wait += clock64() - tw;
-      if (!ok) {
+      if (spins > SPIN_CAP_SLEEP) {
         if (lane == 0) {
           set_status(R, ST_TIMEOUT, 20);
           *(volatile unsigned*)&sm.abort = 1u;
         }
         break;
       }
-      __syncwarp();
       __threadfence_block();
+      W.t_wait += clock64() - tw;
       const int x = sm.pxyz[slot][0], y = sm.pxyz[slot][1], z = sm.pxyz[slot][2];
       const unsigned cid = (unsigned)sm.pxyz[slot][3];
+      const unsigned c0 = sm.pf_c0[slot];
       if (lane < 7) {
         CD mine = sm.pf[slot][lane];
         if (!mine.out) {
-          const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
-          const unsigned fid = lane == 0 ? cid : lane == 1 ? cid - (unsigned)R.PX : lane == 2 ? cid + (unsigned)R.PX
-                             : lane == 3 ? cid + 1u : lane == 4 ? cid - 1u : lane == 5 ? cid + pxy : cid - pxy;
-          unsigned char m;
-          float p;
-          if (fwd_lookup_t(W, W.ft, fid, m, p) || fwd_lookup_t(W, W.ft ^ 1, fid, m, p)) {
-            mine.mat = m;
-            mine.part = p;
-            // a brick materialised since the fetch: take the slot now
-            if (mine.slot == NOSLOT) {
-              unsigned g = R.grid[mine.gi];
-              if (g >= 256u) mine.slot = g - 256u;
-            }
-            sm.pf[slot][lane] = mine;
-          }
+          const int fx = x + ox, fy = y + oy, fz = z + oz;
+          if (!fwd_patch(sm.fwd, cid + oid, fx, fy, fz, c0, mine)) mine = load_cell(R, ring, fx, fy, fz);
+          sm.pf[slot][lane] = mine;
         }
       }
       __syncwarp();
       const long long t1 = clock64();
       W.t_top += t1 - tw;
+      W.seq = r + 1u;
       process_cell(R, W, S, x, y, z, sm.pf[slot]);
       __syncwarp();
       const long long t2 = clock64();
@@ -438,9 +414,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       if (lane == 0) *(volatile unsigned*)&sm.consumed = r + 1u;
       W.t_tail += clock64() - t2;
     }
-    W.fwd_key = nullptr;
-    W.fwd_val = nullptr;
-    W.fwd_part = nullptr;
+    W.fwd = nullptr;
     long long pd = W.pdelta;  // lane-local partial-count deltas
     for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
     W.pdelta = pd;
@@ -462,22 +436,18 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     const unsigned NP = (unsigned)tune.producers;
     const unsigned depth = (unsigned)tune.depth;
     for (unsigned r = warp - 1; r < n; r += NP) {
-      // wait (lane 0, bounded) until the ring slot of cell r is free
-      unsigned ok = 1u;
-      if (lane == 0) {
-        unsigned long long spins = 0;
-        while (*(volatile unsigned*)&sm.consumed + depth <= r) {
-          if (*(volatile unsigned*)&sm.abort || ++spins > SPIN_CAP_SLEEP) {
-            ok = 0u;
-            break;
-          }
-          __nanosleep(200);  // yield issue slots to the sweep warp
+      // wait (bounded) until the ring slot of cell r is free; every lane reads the same words
+      unsigned long long spins = 0;
+      unsigned c0;
+      bool ok = true;
+      while ((c0 = *(volatile unsigned*)&sm.consumed) + depth <= r) {
+        if (*(volatile unsigned*)&sm.abort || ++spins > SPIN_CAP_SLEEP) {
+          ok = false;
+          break;
         }
-        __threadfence_block();
+        __nanosleep(200);  // yield issue slots to the sweep warp
       }
-      ok = __shfl_sync(FULLMASK, ok, 0);
       if (!ok) break;
-      __syncwarp();
       __threadfence_block();
       int x, y, z;
       const unsigned cid = key_to_id(R, R.cells[r], flip);
@@ -490,6 +460,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
         sm.pxyz[r % PF_RING][1] = y;
         sm.pxyz[r % PF_RING][2] = z;
         sm.pxyz[r % PF_RING][3] = (int)cid;
+        sm.pf_c0[r % PF_RING] = c0;
       }
       __syncwarp();
       __threadfence_block();
@@ -591,7 +562,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      Smem S{sm.vis, sm.pq, ring};
+      Smem S{sm.vis, sm.pq, ring, sm.pv};
       W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;

@@ -32,7 +32,7 @@ def _current_stream() -> int:
 def _sim_stream(sim, torch):
     """A torch stream context on the sim's own stream, so tensors made for the sim's kernels are
     ordered with them."""
-    return torch.cuda.stream(torch.cuda.ExternalStream(sim.stream()))
+    return torch.cuda.stream(torch.cuda.ExternalStream(sim.stream))
 
 
 def _sig():
@@ -155,7 +155,7 @@ def features(sim, torch):
     rc = L.vf_fluid_proposal_features(sim.h, C.c_void_p(x.data_ptr()), x.shape[0], C.byref(n))
     if rc:
         raise VfError(rc, "proposal_features")
-    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream()))
+    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream))
     x.record_stream(torch.cuda.current_stream())
     return x[: n.value], n.value
 
@@ -167,7 +167,7 @@ def labels(sim, since_tick: int, nslots: int, torch):
     rc = L.vf_fluid_proposal_labels(sim.h, since_tick, C.c_void_p(y.data_ptr()), nslots)
     if rc:
         raise VfError(rc, "proposal_labels")
-    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream()))
+    torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(sim.stream))
     y.record_stream(torch.cuda.current_stream())
     return y[:nslots]
 
@@ -177,7 +177,7 @@ def stage(sim, prob, threshold: float = 0.5) -> int:
     stream; the sim's stream waits for it)."""
     import torch
 
-    torch.cuda.ExternalStream(sim.stream()).wait_stream(torch.cuda.current_stream())
+    torch.cuda.ExternalStream(sim.stream).wait_stream(torch.cuda.current_stream())
     L = _sig()
     n = C.c_uint64()
     rc = L.vf_fluid_stage_bricks(sim.h, C.c_void_p(prob.data_ptr()), prob.shape[0], threshold, C.byref(n))
