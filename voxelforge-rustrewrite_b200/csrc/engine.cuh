@@ -161,7 +161,7 @@ __host__ __device__ inline unsigned grid_index(const Region& R, int ix, int iy, 
 }
 
 // One cell as the rules see it.
-struct CD {
+struct __align__(16) CD {
   float part;       // partial volume (0 = none)
   unsigned slot;    // atlas slot of the brick, NOSLOT when the brick is a uniform grid value
   unsigned gi;      // grid index

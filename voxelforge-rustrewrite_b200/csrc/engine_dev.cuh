@@ -97,6 +97,9 @@ struct WS {
   // (sorted index + 1) of the cell the sweep is processing
   struct FwdEntry* fwd;
   unsigned seq;
+  // grid words the sweep has read or published (null outside the sweep): GCACHE entries of
+  // grid index << 32 | grid word, one 64-bit store each so that an entry is never torn
+  unsigned long long* gc;
   unsigned long long t_wait, t_pull, t_act, t_write, t_top, t_pc, t_tail;  // cycle counters (profiling)
 };
 
@@ -130,18 +133,6 @@ __device__ __forceinline__ void fwd_insert(WS& W, unsigned id, int x, int y, int
   W.fwd[fwd_index(x, y, z)] = e;
 }
 
-// Patch a prefetched cell (fetched when c0 cells were finished). Returns false when the value
-// cannot be told from the table and must be re-read from memory.
-__device__ __forceinline__ bool fwd_patch(const FwdEntry* tab, unsigned id, int x, int y, int z, unsigned c0, CD& c) {
-  const FwdEntry e = tab[fwd_index(x, y, z)];
-  if ((e.meta & 0xFFFFu) <= c0) return true;  // not written since the fetch
-  if (e.tag != id) return false;
-  c.mat = (unsigned char)(e.meta >> 16);
-  c.part = e.part;
-  c.slot = e.slot;
-  return true;
-}
-
 constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
 
 struct Smem {
@@ -159,7 +150,9 @@ __device__ __forceinline__ void set_status(const Region& R, int st, unsigned inf
 // Bricks that are uniform grid values get an atlas slot before their first write (the
 // reference's SparseVolume::materialize, sparse_volume.rs:250-266; partial pages, fluid.rs:108-128).
 // Lanes with `need` name a grid index; one leader per distinct index allocates, the warp fills.
-__device__ void materialize_lanes(const Region& R, bool need, unsigned gi, unsigned& slot) {
+constexpr unsigned GCACHE = 1024;  // grid-word cache entries of the sweep (direct-mapped by grid index)
+
+__device__ void materialize_lanes(const Region& R, bool need, unsigned gi, unsigned& slot, unsigned long long* gc = nullptr) {
   const unsigned lane = lane_id();
   unsigned key = need ? gi : (0xFFFFFFFFu - lane);
   unsigned peers = __match_any_sync(FULLMASK, key);
@@ -201,7 +194,11 @@ __device__ void materialize_lanes(const Region& R, bool need, unsigned gi, unsig
   // publish the slot after its fill (release): prefetching warps read the grid word first and
   // then the atlas, with a fence in between
   __threadfence_block();
-  if (leader && s != NOSLOT && g < 256u) *(volatile unsigned*)(R.grid + gi) = 256u + s;
+  if (leader && s != NOSLOT && g < 256u) {
+    *(volatile unsigned*)(R.grid + gi) = 256u + s;
+    unsigned long long* e = gc ? gc + (gi & (GCACHE - 1u)) : nullptr;
+    if (e && (unsigned)(*e >> 32) == gi) *e = ((unsigned long long)gi << 32) | (256u + s);
+  }
   int src = need ? (__ffs(peers) - 1) : (int)lane;
   unsigned s2 = __shfl_sync(FULLMASK, s, src);
   if (need) slot = s2;
@@ -292,7 +289,7 @@ __device__ __forceinline__ unsigned log_append(const Region& R, unsigned* log, u
 __device__ bool warp_set_volume(const Region& R, WS& W, bool w, CD& c, int x, int y, int z, float vol) {
   const long long t0 = fine_clock();
   bool need = w && set_volume_needs_slot(c, vol);
-  if (__any_sync(FULLMASK, need)) materialize_lanes(R, need, c.gi, c.slot);
+  if (__any_sync(FULLMASK, need)) materialize_lanes(R, need, c.gi, c.slot, W.gc);
   bool ch = false;
   const unsigned id = (w && in_dom(R, x, y, z)) ? dom_id(R, x, y, z) : 0u;
   if (w) {
@@ -462,6 +459,38 @@ __device__ __forceinline__ bool vis_insert(unsigned long long* vis, unsigned id,
   }
 }
 
+// load_cell for the sweep's pressure search: the grid word comes from the sweep's cache when it
+// holds it (only the sweep warp publishes grid words during a sweep, and it updates the cache).
+__device__ __forceinline__ CD load_cell_gc(const Region& R, const WS& W, const int* ring, int x, int y, int z) {
+  if (!W.gc) return load_cell(R, ring, x, y, z);
+  CD c;
+  c.part = 0.0f;
+  c.slot = NOSLOT;
+  c.gi = 0;
+  c.mat = 0;
+  c.out = outside(R, ring, x, y, z);
+  if (c.out) return c;
+  c.gi = grid_index(R, x >> 3, y >> 3, z >> 3);
+  const unsigned h = c.gi & (GCACHE - 1u);
+  const unsigned long long e = W.gc[h];
+  unsigned g;
+  if ((unsigned)(e >> 32) == c.gi) {
+    g = (unsigned)e;
+  } else {
+    g = R.grid[c.gi];
+    W.gc[h] = ((unsigned long long)c.gi << 32) | g;
+  }
+  if (g < 256u) {
+    c.mat = (unsigned char)g;
+    return c;
+  }
+  c.slot = g - 256u;
+  size_t o = (size_t)c.slot * 512u + local_index(x, y, z);
+  c.mat = R.amat[o];
+  c.part = R.avol[o];
+  return c;
+}
+
 // D of pressure_pull (fluid.rs:512): up, +x, -x, +z, -z.
 __device__ __forceinline__ void dir5(int d, int& dx, int& dy, int& dz) {
   dx = (d == 1) - (d == 2);
@@ -536,7 +565,7 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
       na = a + dx;
       nb = b + dy;
       nc = c + dz;
-      cd = load_cell(R, S.ring, na, nb, nc);
+      cd = load_cell_gc(R, W, S.ring, na, nb, nc);
     }
     // surface test of each entry on its up neighbour (fluid.rs:534-535)
     const bool win = act && d == 0u && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f) && b > y && here > 0.0f;
@@ -584,9 +613,84 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
 
 // --------------------------------------------------------------------------- one cell
 // The body of FluidSim::tick's loop (fluid.rs:584-650) for the cell (x, y, z).
-// `pre` (optional): the footprint as prefetched and store-forwarded by the sweep, in shared
-// memory (7 cells); without it the warp loads the footprint itself.
-__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z, const CD* pre = nullptr) {
+// The flow part of a cell's update (fluid.rs:606-650 after the pressure pull) from its footprint
+// and its volume `vol` (> 0) at that point: 1. fall into the free capacity below, 2. share with
+// lower sides when supported, 3. evaporate crumbs. Written as selects: every side's flow depends
+// only on `here` (the volume after the fall) and that side's volume, so the four decisions are
+// independent; only the running volume subtracts them in side order.
+struct CellPlan {
+  float vol;          // the cell's volume afterwards (before the write-back test)
+  float below_new;    // the cell below's new volume when w_below
+  float side_new[4];  // +x, -x, +z, -z new volumes when their bit of wside is set
+  bool w_below;
+  unsigned wside;     // bit i: side i is written
+  unsigned amask;     // activation slots 2 (below) and 3..6 (sides)
+};
+
+__device__ __forceinline__ CellPlan plan_flow(const CD* fp, float vol) {
+  const float FULL = full_level();
+  CellPlan P;
+  const bool below_solid = cd_solid(fp[1]);
+  const float bv = cd_volume(fp[1]);
+  const float ff = fminf(vol, __fsub_rn(1.0f, bv));
+  P.w_below = !below_solid && ff > 1e-6f;
+  P.below_new = __fadd_rn(bv, ff);
+  vol = P.w_below ? __fsub_rn(vol, ff) : vol;
+  const float below_after = P.w_below ? (P.below_new >= FULL ? 1.0f : P.below_new) : bv;
+  const bool spread = vol > MIN_SPREAD && (below_solid || below_after >= FULL);
+  const float here = vol;
+  P.wside = 0u;
+  P.amask = P.w_below ? (1u << 2) : 0u;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const bool open = !cd_solid(fp[3 + i]);
+    const float nv = open ? cd_volume(fp[3 + i]) : 0.0f;
+    const float f = __fmul_rn(__fsub_rn(here, nv), 0.2f);
+    const bool ok = spread && open && !(nv >= here) && !(f < MIN_FLOW) && !(__fsub_rn(here, f) < MIN_SPREAD * 0.5f);
+    P.side_new[i] = __fadd_rn(nv, f);
+    P.wside |= ok ? (1u << i) : 0u;
+    vol = ok ? __fsub_rn(vol, f) : vol;
+    P.amask |= (ok && f > SLEEP) ? (1u << (3 + i)) : 0u;
+  }
+  P.vol = vol < EVAPORATE ? 0.0f : vol;
+  return P;
+}
+
+// Does the pressure pull of a cell at (x, y, z) have a start cell (a full up/side neighbour with
+// x, z >= 0; fluid.rs:518-525)? Without one the pull examines nothing and takes nothing.
+__device__ __forceinline__ bool pull_has_start(const CD* fp, int x, int z) {
+  const float FULL = full_level();
+  bool any = false;
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const CD& c = fp[2 + d];  // up, +x, -x, +z, -z (the pull's direction order)
+    const int a = x + (d == 1) - (d == 2), cc = z + (d == 3) - (d == 4);
+    any |= a >= 0 && cc >= 0 && !cd_solid(c) && cd_volume(c) >= FULL;
+  }
+  return any;
+}
+
+// Quiet-cell classification for the sweep's prefetchers. Bit 0: processing the cell with this
+// footprint writes nothing, activates nothing and seeds nothing (a solid cell without a partial
+// entry; or a cell whose pull, if it attempts one, has no start cell and whose flow plan changes
+// no volume by more than 1e-7); bit 1: the cell attempts a pull (counted against the tick's
+// budget). Everything else goes through process_cell.
+constexpr unsigned QUIET = 1u, QUIET_PULL = 2u;
+__device__ __forceinline__ unsigned classify_quiet(const CD* fp, int x, int z) {
+  if (cd_solid(fp[0])) return (fp[0].slot != NOSLOT && fp[0].part > 0.0f) ? 0u : QUIET;
+  const float v0 = cd_volume(fp[0]);
+  const bool attempt = v0 < full_level();
+  if (attempt && pull_has_start(fp, x, z)) return 0u;
+  const unsigned pbit = attempt ? QUIET_PULL : 0u;
+  if (v0 <= 0.0f) return QUIET | pbit;
+  const CellPlan P = plan_flow(fp, v0);
+  const float dv = fabsf(__fsub_rn(P.vol, v0));
+  const bool quiet = !P.w_below && P.wside == 0u && !(dv > 1e-7f);
+  return quiet ? (QUIET | pbit) : 0u;
+}
+
+// `pre`: the footprint as prefetched and store-forwarded by the sweep, in shared memory (7 cells).
+__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z, const CD* pre) {
   const unsigned lane = lane_id();
   const float FULL = full_level();
   // footprint: 0 self, 1 below, 2 up, 3 +x, 4 -x, 5 +z, 6 -z
@@ -597,19 +701,10 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   else if (lane == 4) fx -= 1;
   else if (lane == 5) fz += 1;
   else if (lane == 6) fz -= 1;
-  CD mine;
   CD fp[7];
-  if (pre) {
 #pragma unroll
-    for (int j = 0; j < 7; ++j) fp[j] = pre[j];
-    mine = lane < 7 ? pre[lane] : CD{0.0f, NOSLOT, 0u, 0, true};
-  } else {
-    if (lane < 7) mine = load_cell(R, S.ring, fx, fy, fz);
-    else mine = CD{0.0f, NOSLOT, 0u, 0, true};
-#pragma unroll
-    for (int j = 0; j < 7; ++j) fp[j] = shfl_cd(mine, j);
-  }
-  const unsigned id = dom_id(R, x, y, z);
+  for (int j = 0; j < 7; ++j) fp[j] = pre[j];
+  CD mine = lane < 7 ? pre[lane] : CD{0.0f, NOSLOT, 0u, 0, true};
   if (cd_solid(fp[0])) {  // fluid.rs:586-589
     if (lane == 0) erase_part(R, mine, local_index(x, y, z), W.pdelta);
     __syncwarp();
@@ -636,50 +731,19 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
     flush_acts(R, W, A);
     return;
   }
-  // 1. fall (fluid.rs:606-614)
-  bool w_below = false;
-  float below_new = 0.0f;
-  const bool below_solid = cd_solid(fp[1]);
-  float below_after = cd_volume(fp[1]);
-  if (!below_solid) {
-    float bv = cd_volume(fp[1]);
-    float f = fminf(vol, __fsub_rn(1.0f, bv));
-    if (f > 1e-6f) {
-      below_new = __fadd_rn(bv, f);
-      w_below = true;
-      vol = __fsub_rn(vol, f);
-      A.slot(2);
-      below_after = below_new >= FULL ? 1.0f : below_new;
-    }
-  }
-  // 2. spread (fluid.rs:617-639)
-  bool w_side[4] = {false, false, false, false};
-  float side_new[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  if (vol > MIN_SPREAD && (below_solid || below_after >= FULL)) {
-    float nv[4];
-    bool open[4];
+  const CellPlan P = plan_flow(fp, vol);
+  vol = P.vol;
+  A.mask |= P.amask;
+  const bool w_below = P.w_below;
+  const float below_new = P.below_new;
+  bool w_side[4];
+  float side_new[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      open[i] = !cd_solid(fp[3 + i]);
-      nv[i] = open[i] ? cd_volume(fp[3 + i]) : 0.0f;
-    }
-    const float here = vol;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      if (!open[i] || nv[i] >= here) continue;
-      float f = __fmul_rn(__fsub_rn(here, nv[i]), 0.2f);
-      if (f < MIN_FLOW || __fsub_rn(here, f) < MIN_SPREAD * 0.5f) continue;
-      side_new[i] = __fadd_rn(nv[i], f);
-      w_side[i] = true;
-      vol = __fsub_rn(vol, f);
-      if (f > SLEEP) {
-        (void)0;
-        A.slot(3 + i);
-      }
-    }
+  for (int i = 0; i < 4; ++i) {
+    w_side[i] = (P.wside >> i) & 1u;
+    side_new[i] = P.side_new[i];
   }
   // 3. evaporate, write back, sleep test (fluid.rs:641-650)
-  if (vol < EVAPORATE) vol = 0.0f;
   const float dv = fabsf(__fsub_rn(vol, v0));
   const bool w_self = dv > 1e-7f;
   // parallel writes into distinct cells: lane 0 self, 1 below, 3..6 sides
@@ -710,7 +774,6 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
     seed_level(R, W, x, y, z);
   }
   flush_acts(R, W, A);
-  (void)id;
 }
 
 // ------------------------------------------------------------------------ level fill

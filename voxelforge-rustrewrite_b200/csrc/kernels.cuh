@@ -142,7 +142,9 @@ struct TickSmem {
   unsigned pf_ready[PF_RING];   // the cell index whose footprint a slot holds
   int pxyz[PF_RING][4];         // the cell's coordinates and domain id
   unsigned pf_c0[PF_RING];      // cells the sweep had finished when the slot's footprint was fetched
+  unsigned pf_quiet[PF_RING];   // classify_quiet of the fetched footprint
   FwdEntry fwd[FWD_SIZE];       // the sweep's latest writes (store forwarding)
+  unsigned long long gc[GCACHE];  // grid-word cache of the sweep's pressure searches
   unsigned consumed;            // cells the sweep has finished
   unsigned abort;               // a wait gave up: every warp leaves the sweep
   unsigned scan[TICK_WARPS + 1];
@@ -168,6 +170,7 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.nact = W.nseed = W.nchg = 0;
   W.fwd = nullptr;
   W.seq = 0;
+  W.gc = nullptr;
   W.t_wait = W.t_pull = W.t_act = W.t_write = W.t_top = W.t_pc = W.t_tail = 0;
 }
 
@@ -364,10 +367,12 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
   }
   for (unsigned i = tid; i < PF_RING; i += TICK_THREADS) sm.pf_ready[i] = 0xFFFFFFFFu;
   for (unsigned i = tid; i < FWD_SIZE; i += TICK_THREADS) sm.fwd[i].meta = 0u;
+  for (unsigned i = tid; i < GCACHE; i += TICK_THREADS) sm.gc[i] = ~0ull;
   __syncthreads();
   if (warp == 0) {
     WS W = sW;
     W.fwd = sm.fwd;
+    W.gc = sm.gc;
     Smem S{sm.vis, sm.pq, ring, sm.pv};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
@@ -394,19 +399,41 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       const int x = sm.pxyz[slot][0], y = sm.pxyz[slot][1], z = sm.pxyz[slot][2];
       const unsigned cid = (unsigned)sm.pxyz[slot][3];
       const unsigned c0 = sm.pf_c0[slot];
+      const unsigned quiet = sm.pf_quiet[slot];
+      // footprint cells the sweep wrote since the fetch: from the forwarding table, or from
+      // memory when another cell's write took the cell's table entry
+      bool touched = false;
       if (lane < 7) {
         CD mine = sm.pf[slot][lane];
-        if (!mine.out) {
-          const int fx = x + ox, fy = y + oy, fz = z + oz;
-          if (!fwd_patch(sm.fwd, cid + oid, fx, fy, fz, c0, mine)) mine = load_cell(R, ring, fx, fy, fz);
+        const int fx = x + ox, fy = y + oy, fz = z + oz;
+        const FwdEntry e = sm.fwd[fwd_index(fx, fy, fz)];
+        if (!mine.out && (e.meta & 0xFFFFu) > c0) {
+          touched = true;
+          if (e.tag == cid + oid) {
+            mine.mat = (unsigned char)(e.meta >> 16);
+            mine.part = e.part;
+            mine.slot = e.slot;
+          } else {
+            mine = load_cell(R, ring, fx, fy, fz);
+          }
           sm.pf[slot][lane] = mine;
         }
       }
+      const bool stale = __any_sync(FULLMASK, touched);
       __syncwarp();
       const long long t1 = clock64();
       W.t_top += t1 - tw;
       W.seq = r + 1u;
-      process_cell(R, W, S, x, y, z, sm.pf[slot]);
+      if (!stale && (quiet & QUIET)) {
+        // nothing to write, activate or seed (classified by the prefetcher on this footprint):
+        // only the pull budget counts the attempt
+        if ((quiet & QUIET_PULL) && W.pulls < MAX_PULLS_PER_TICK) {
+          W.pulls += 1;
+          W.pull_attempts += 1;
+        }
+      } else {
+        process_cell(R, W, S, x, y, z, sm.pf[slot]);
+      }
       __syncwarp();
       const long long t2 = clock64();
       W.t_pc += t2 - t1;
@@ -415,6 +442,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       W.t_tail += clock64() - t2;
     }
     W.fwd = nullptr;
+    W.gc = nullptr;
     long long pd = W.pdelta;  // lane-local partial-count deltas
     for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
     W.pdelta = pd;
@@ -452,19 +480,26 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       int x, y, z;
       const unsigned cid = key_to_id(R, R.cells[r], flip);
       dom_xyz(R, cid, x, y, z);
+      const unsigned s = r % PF_RING;
       if (lane < 7) {
         int fx = x + (lane == 3) - (lane == 4), fy = y - (lane == 1) + (lane == 2), fz = z + (lane == 5) - (lane == 6);
-        sm.pf[r % PF_RING][lane] = load_cell_acq(R, ring, fx, fy, fz);
+        sm.pf[s][lane] = load_cell_acq(R, ring, fx, fy, fz);
       } else if (lane == 7) {
-        sm.pxyz[r % PF_RING][0] = x;
-        sm.pxyz[r % PF_RING][1] = y;
-        sm.pxyz[r % PF_RING][2] = z;
-        sm.pxyz[r % PF_RING][3] = (int)cid;
-        sm.pf_c0[r % PF_RING] = c0;
+        sm.pxyz[s][0] = x;
+        sm.pxyz[s][1] = y;
+        sm.pxyz[s][2] = z;
+        sm.pxyz[s][3] = (int)cid;
+        sm.pf_c0[s] = c0;
       }
       __syncwarp();
+      CD fq[7];
+#pragma unroll
+      for (int j = 0; j < 7; ++j) fq[j] = sm.pf[s][j];
+      const unsigned q = classify_quiet(fq, x, z);
+      if (lane == 0) sm.pf_quiet[s] = q;
+      __syncwarp();
       __threadfence_block();
-      if (lane == 0) *(volatile unsigned*)&sm.pf_ready[r % PF_RING] = r;
+      if (lane == 0) *(volatile unsigned*)&sm.pf_ready[s] = r;
     }
   }
   __syncthreads();
