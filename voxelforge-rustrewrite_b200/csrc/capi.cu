@@ -771,9 +771,20 @@ int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
-  if (out16) std::memcpy(out16, h->hctl->prof, sizeof(h->hctl->prof));
+  if (out16) std::memcpy(out16, h->hctl->prof, 16 * sizeof(uint64_t));
   return VF_OK;
 }
+
+#ifdef VF_FINE_PROFILE
+// Fine-profiling builds only: all 24 counters (the 16 phases and the per-call counters).
+extern "C" int vf_fluid_profile_fine(vf_fluid* h, uint64_t* out24) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (out24) std::memcpy(out24, h->hctl->prof, 24 * sizeof(uint64_t));
+  return VF_OK;
+}
+#endif
 
 // ---------------------------------------------------------------- learned wake proposal
 static int proposal_buffers(vf_fluid* h) {

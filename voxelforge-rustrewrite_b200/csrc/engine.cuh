@@ -55,7 +55,11 @@ struct Ctl {
   // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear
+#ifdef VF_FINE_PROFILE
+  unsigned long long prof[24];  // + per-call counters of the fine-profiling build
+#else
   unsigned long long prof[16];
+#endif
 };
 constexpr int NPROF = 16;
 

@@ -101,6 +101,9 @@ struct WS {
   // grid index << 32 | grid word, one 64-bit store each so that an entry is never torn
   unsigned long long* gc;
   unsigned long long t_wait, t_pull, t_act, t_write, t_top, t_pc, t_tail;  // cycle counters (profiling)
+#ifdef VF_FINE_PROFILE
+  unsigned long long f_pre, f_plan, f_seed, n_pc, n_quiet, n_rounds;
+#endif
 };
 
 // Store forwarding for the prefetching sweep: a direct-mapped table of the sweep's latest writes.
@@ -137,9 +140,8 @@ constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
 
 struct Smem {
   unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
-  unsigned* pq;             // PRESS_QCAP
   const int* ring;
-  float* pv;                // PRESS_QCAP: volume of each queued cell when it was queued
+  int4* pq;                 // PRESS_QCAP queued cells: x, y, z and the volume (bits) seen when queued
 };
 
 __device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
@@ -541,9 +543,10 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
   if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
   __syncwarp();
   if (ok) {
+    int dx, dy, dz;
+    dir5((int)lane, dx, dy, dz);
     const unsigned pos = (unsigned)__popc(bm & lanemask_lt());
-    S.pq[pos] = nid;
-    S.pv[pos] = nvol;
+    S.pq[pos] = make_int4(x + dx, y + dy, z + dz, __float_as_int(nvol));
     vis_insert(S.vis, nid, W.epoch);
   }
   __syncwarp();
@@ -557,9 +560,11 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     float here = 0.0f;
     CD cd = CD{0.0f, NOSLOT, 0u, 0, true};
     if (act) {
-      const unsigned e = S.pq[i + j];
-      here = S.pv[i + j];
-      dom_xyz(R, e, a, b, c);
+      const int4 e = S.pq[i + j];
+      a = e.x;
+      b = e.y;
+      c = e.z;
+      here = __int_as_float(e.w);
       int dx, dy, dz;
       dir5((int)d, dx, dy, dz);
       na = a + dx;
@@ -598,13 +603,13 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     const unsigned nm = __ballot_sync(FULLMASK, isnew);
     if (isnew) {
       const unsigned pos = qlen + (unsigned)__popc(nm & lanemask_lt());
-      if (pos < PRESS_QCAP) {
-        S.pq[pos] = id;
-        S.pv[pos] = cd_volume(cd);
-      }
+      if (pos < PRESS_QCAP) S.pq[pos] = make_int4(na, nb, nc, __float_as_int(cd_volume(cd)));
     }
     qlen += (unsigned)__popc(nm);
     i += k;
+#ifdef VF_FINE_PROFILE
+    W.n_rounds += 1;
+#endif
     __syncwarp();
   }
   W.bfs_visits += i;
@@ -689,22 +694,16 @@ __device__ __forceinline__ unsigned classify_quiet(const CD* fp, int x, int z) {
   return quiet ? (QUIET | pbit) : 0u;
 }
 
-// `pre`: the footprint as prefetched and store-forwarded by the sweep, in shared memory (7 cells).
-__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z, const CD* pre) {
+// fp: the footprint (0 self, 1 below, 2 up, 3 +x, 4 -x, 5 +z, 6 -z) as prefetched and
+// store-forwarded by the sweep, the same on every lane; lanes 0..6 also hold their own cell
+// (`mine`, at fx, fy, fz).
+__device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int z, int fx, int fy, int fz, const CD (&fp)[7], CD mine) {
+#ifdef VF_FINE_PROFILE
+  const long long f0 = clock64();
+  W.n_pc += 1;
+#endif
   const unsigned lane = lane_id();
   const float FULL = full_level();
-  // footprint: 0 self, 1 below, 2 up, 3 +x, 4 -x, 5 +z, 6 -z
-  int fx = x, fy = y, fz = z;
-  if (lane == 1) fy -= 1;
-  else if (lane == 2) fy += 1;
-  else if (lane == 3) fx += 1;
-  else if (lane == 4) fx -= 1;
-  else if (lane == 5) fz += 1;
-  else if (lane == 6) fz -= 1;
-  CD fp[7];
-#pragma unroll
-  for (int j = 0; j < 7; ++j) fp[j] = pre[j];
-  CD mine = lane < 7 ? pre[lane] : CD{0.0f, NOSLOT, 0u, 0, true};
   if (cd_solid(fp[0])) {  // fluid.rs:586-589
     if (lane == 0) erase_part(R, mine, local_index(x, y, z), W.pdelta);
     __syncwarp();
@@ -714,6 +713,9 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   A.reset(x, y, z);
   float vol = cd_volume(fp[0]);
   const float v0 = vol;
+#ifdef VF_FINE_PROFILE
+  W.f_pre += clock64() - f0;
+#endif
   // 0. pressure (fluid.rs:594-601)
   if (vol < FULL && W.pulls < MAX_PULLS_PER_TICK) {
     const long long tp = fine_clock();
@@ -731,8 +733,14 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
     flush_acts(R, W, A);
     return;
   }
+#ifdef VF_FINE_PROFILE
+  const long long f1 = clock64();
+#endif
   const CellPlan P = plan_flow(fp, vol);
   vol = P.vol;
+#ifdef VF_FINE_PROFILE
+  W.f_plan += clock64() - f1;
+#endif
   A.mask |= P.amask;
   const bool w_below = P.w_below;
   const float below_new = P.below_new;
@@ -770,8 +778,14 @@ __device__ void process_cell(const Region& R, WS& W, Smem& S, int x, int y, int 
   }
   if (__any_sync(FULLMASK, w)) W.changed |= warp_set_volume(R, W, w, mine, fx, fy, fz, wv);
   if (dv > SLEEP) {
+#ifdef VF_FINE_PROFILE
+    const long long f2 = clock64();
+#endif
     A.slot(7);
     seed_level(R, W, x, y, z);
+#ifdef VF_FINE_PROFILE
+    W.f_seed += clock64() - f2;
+#endif
   }
   flush_acts(R, W, A);
 }

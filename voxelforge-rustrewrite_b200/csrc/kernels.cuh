@@ -134,8 +134,7 @@ constexpr unsigned long long SPIN_CAP_SLEEP = 1ull << 23;  // waits with a nanos
 struct TickSmem {
   unsigned hist[TICK_WARPS * 256];
   unsigned sred[2 * 256 + 64];
-  unsigned pq[PRESS_QCAP];
-  float pv[PRESS_QCAP];
+  int4 pq[PRESS_QCAP];
   unsigned long long vis[VIS_CAP];
   int ring[3 * 16 * 16];
   CD pf[PF_RING][7];            // prefetched footprints (self, below, up, +x, -x, +z, -z)
@@ -172,6 +171,9 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.seq = 0;
   W.gc = nullptr;
   W.t_wait = W.t_pull = W.t_act = W.t_write = W.t_top = W.t_pc = W.t_tail = 0;
+#ifdef VF_FINE_PROFILE
+  W.f_pre = W.f_plan = W.f_seed = W.n_pc = W.n_quiet = W.n_rounds = 0;
+#endif
 }
 
 // Load a cell for the prefetch ring: the grid word is read with a fence after it, pairing with
@@ -373,7 +375,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     WS W = sW;
     W.fwd = sm.fwd;
     W.gc = sm.gc;
-    Smem S{sm.vis, sm.pq, ring, sm.pv};
+    Smem S{sm.vis, ring, sm.pq};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
     const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
@@ -431,8 +433,15 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
           W.pulls += 1;
           W.pull_attempts += 1;
         }
+#ifdef VF_FINE_PROFILE
+        W.n_quiet += 1;
+#endif
       } else {
-        process_cell(R, W, S, x, y, z, sm.pf[slot]);
+        CD fp[7];
+#pragma unroll
+        for (int j = 0; j < 7; ++j) fp[j] = sm.pf[slot][j];
+        const CD mine = lane < 7 ? sm.pf[slot][lane] : CD{0.0f, NOSLOT, 0u, 0, true};
+        process_cell(R, W, S, x, y, z, x + ox, y + oy, z + oz, fp, mine);
       }
       __syncwarp();
       const long long t2 = clock64();
@@ -457,6 +466,15 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       c.prof[13] += W.t_pc;
       c.prof[14] += W.t_tail;
       sW.t_wait = sW.t_pull = sW.t_act = sW.t_write = sW.t_top = sW.t_pc = sW.t_tail = 0;
+#ifdef VF_FINE_PROFILE
+      c.prof[16] += W.f_pre;
+      c.prof[17] += W.f_plan;
+      c.prof[18] += W.f_seed;
+      c.prof[19] += W.n_pc;
+      c.prof[20] += W.n_quiet;
+      c.prof[21] += W.n_rounds;
+      sW.f_pre = sW.f_plan = sW.f_seed = sW.n_pc = sW.n_quiet = sW.n_rounds = 0;
+#endif
     }
     __syncwarp();
   } else if (warp <= (unsigned)tune.producers) {
@@ -597,7 +615,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      Smem S{sm.vis, sm.pq, ring, sm.pv};
+      Smem S{sm.vis, ring, sm.pq};
       W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
