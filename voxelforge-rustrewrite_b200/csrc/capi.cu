@@ -776,12 +776,12 @@ int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
 }
 
 #ifdef VF_FINE_PROFILE
-// Fine-profiling builds only: all 24 counters (the 16 phases and the per-call counters).
-extern "C" int vf_fluid_profile_fine(vf_fluid* h, uint64_t* out24) {
+// Fine-profiling builds only: all 32 counters (the 16 phases and the per-call counters).
+extern "C" int vf_fluid_profile_fine(vf_fluid* h, uint64_t* out32) {
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
-  if (out24) std::memcpy(out24, h->hctl->prof, 24 * sizeof(uint64_t));
+  if (out32) std::memcpy(out32, h->hctl->prof, 32 * sizeof(uint64_t));
   return VF_OK;
 }
 #endif

@@ -34,7 +34,11 @@ constexpr uint32_t MAX_LEVEL_SEEDS = 4096;
 constexpr uint32_t NOSLOT = 0xFFFFFFFFu;
 // Press-BFS queue bound: 5 start cells + 5 pushes per examined entry, 512 entries examined.
 constexpr uint32_t PRESS_QCAP = 5 + 5 * PRESSURE_SEARCH + 8;
-constexpr uint32_t VIS_CAP = 8192;  // smem visited hash (load <= 32%)
+constexpr uint32_t VIS_CAP = 4096;  // smem visited hash for cells outside the bitmap box (load <= 63%)
+// Visited bitmap of a pressure search: a box of 64 x 64 (x, z around the start) x 64 (y from the
+// start up) cells, one bit each; cells outside it use the hash.
+constexpr int VB_SIDE = 64;
+constexpr uint32_t VB_WORDS = VB_SIDE * VB_SIDE * VB_SIDE / 32;
 
 // status codes written to Ctl::status by device code (mirrors VF_ERR_*)
 constexpr int ST_OK = 0;
@@ -56,7 +60,7 @@ struct Ctl {
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear
 #ifdef VF_FINE_PROFILE
-  unsigned long long prof[24];  // + per-call counters of the fine-profiling build
+  unsigned long long prof[32];  // + per-call counters of the fine-profiling build
 #else
   unsigned long long prof[16];
 #endif

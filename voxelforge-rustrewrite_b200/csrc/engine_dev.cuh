@@ -102,7 +102,7 @@ struct WS {
   unsigned long long* gc;
   unsigned long long t_wait, t_pull, t_act, t_write, t_top, t_pc, t_tail;  // cycle counters (profiling)
 #ifdef VF_FINE_PROFILE
-  unsigned long long f_pre, f_plan, f_seed, n_pc, n_quiet, n_rounds;
+  unsigned long long f_pre, f_plan, f_seed, n_pc, n_quiet, n_rounds, f_bload, f_bexp, f_match, f_vis;
 #endif
 };
 
@@ -142,6 +142,8 @@ struct Smem {
   unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
   const int* ring;
   int4* pq;                 // PRESS_QCAP queued cells: x, y, z and the volume (bits) seen when queued
+  unsigned* vb;             // VB_WORDS: visited bitmap of the search box (all zero between searches)
+  unsigned* vtl;            // PRESS_QCAP: bitmap words the current search set (cleared at its end)
 };
 
 __device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
@@ -493,6 +495,32 @@ __device__ __forceinline__ CD load_cell_gc(const Region& R, const WS& W, const i
   return c;
 }
 
+// Visited test-and-insert of a pressure search started at (x0, y0, z0), warp-collective: lanes
+// with `want` insert their cell (distinct cells; at most one lane per cell). Cells in the bitmap
+// box take one atomicOr; the lane that finds its word empty adds the word to the touched list,
+// which the search's end clears. Cells outside the box use the epoch-tagged hash. Returns "new".
+__device__ __forceinline__ bool visit(const Smem& S, unsigned epoch, unsigned& ntouch, int x0, int y0, int z0, bool want, int a, int b, int c,
+                                      unsigned id) {
+  const unsigned lx = (unsigned)(a - x0 + VB_SIDE / 2), ly = (unsigned)(b - y0), lz = (unsigned)(c - z0 + VB_SIDE / 2);
+  const bool inbox = want && lx < (unsigned)VB_SIDE && ly < (unsigned)VB_SIDE && lz < (unsigned)VB_SIDE;
+  bool isnew = false, first = false;
+  unsigned word = 0;
+  if (inbox) {
+    const unsigned bit = (ly * VB_SIDE + lz) * VB_SIDE + lx;
+    const unsigned m = 1u << (bit & 31u);
+    word = bit >> 5;
+    const unsigned old = atomicOr(&S.vb[word], m);
+    first = old == 0u;
+    isnew = !(old & m);
+  } else if (want) {
+    isnew = vis_insert(S.vis, id, epoch);
+  }
+  const unsigned fm = __ballot_sync(FULLMASK, first);
+  if (first) S.vtl[ntouch + (unsigned)__popc(fm & lanemask_lt())] = word;
+  ntouch += (unsigned)__popc(fm);
+  return isnew;
+}
+
 // D of pressure_pull (fluid.rs:512): up, +x, -x, +z, -z.
 __device__ __forceinline__ void dir5(int d, int& dx, int& dy, int& dz) {
   dx = (d == 1) - (d == 2);
@@ -540,20 +568,26 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     __syncwarp();
     W.epoch = 1u;
   }
-  if (lane == 0) vis_insert(S.vis, dom_id(R, x, y, z), W.epoch);
+  unsigned ntouch = 0;
+  visit(S, W.epoch, ntouch, x, y, z, lane == 0, x, y, z, dom_id(R, x, y, z));
   __syncwarp();
-  if (ok) {
-    int dx, dy, dz;
-    dir5((int)lane, dx, dy, dz);
-    const unsigned pos = (unsigned)__popc(bm & lanemask_lt());
-    S.pq[pos] = make_int4(x + dx, y + dy, z + dz, __float_as_int(nvol));
-    vis_insert(S.vis, nid, W.epoch);
+  {
+    int dx = 0, dy = 0, dz = 0;
+    if (lane < 5) dir5((int)lane, dx, dy, dz);
+    if (ok) {
+      const unsigned pos = (unsigned)__popc(bm & lanemask_lt());
+      S.pq[pos] = make_int4(x + dx, y + dy, z + dz, __float_as_int(nvol));
+    }
+    visit(S, W.epoch, ntouch, x, y, z, ok, x + dx, y + dy, z + dz, nid);
   }
   __syncwarp();
   const unsigned j = lane / 5u, d = lane - 5u * (lane / 5u);
   unsigned side = 0, i = 0;
   float got = 0.0f;
   while (i < qlen && i < PRESSURE_SEARCH) {
+#ifdef VF_FINE_PROFILE
+    const long long b0 = clock64();
+#endif
     const unsigned k = min(PB, min(qlen - i, PRESSURE_SEARCH - i));
     const bool act = j < k;
     int a = 0, b = 0, c = 0, na = 0, nb = 0, nc = 0;
@@ -575,6 +609,10 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     // surface test of each entry on its up neighbour (fluid.rs:534-535)
     const bool win = act && d == 0u && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f) && b > y && here > 0.0f;
     const unsigned wm = __ballot_sync(FULLMASK, win);
+#ifdef VF_FINE_PROFILE
+    const long long b1 = clock64();
+    W.f_bload += b1 - b0;
+#endif
     if (wm) {
       const int wl = __ffs(wm) - 1;
       const int wa = __shfl_sync(FULLMASK, a, wl), wb = __shfl_sync(FULLMASK, b, wl), wc = __shfl_sync(FULLMASK, c, wl);
@@ -597,9 +635,19 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     if (sc && side + (unsigned)__popc(sm & lanemask_lt()) + 1u > 24u) cand = false;
     side += (unsigned)__popc(sm);
     const unsigned id = cand ? dom_id(R, na, nb, nc) : (0xFFFFFFFFu - lane);
+#ifdef VF_FINE_PROFILE
+    const long long b2 = clock64();
+#endif
     const unsigned peers = __match_any_sync(FULLMASK, id);
-    bool isnew = false;
-    if (cand && !(peers & lanemask_lt())) isnew = vis_insert(S.vis, id, W.epoch);
+#ifdef VF_FINE_PROFILE
+    const long long b3 = clock64();
+    W.f_match += b3 - b2;
+#endif
+    const bool isnew = visit(S, W.epoch, ntouch, x, y, z, cand && !(peers & lanemask_lt()), na, nb, nc, id);
+#ifdef VF_FINE_PROFILE
+    __syncwarp();
+    W.f_vis += clock64() - b3;
+#endif
     const unsigned nm = __ballot_sync(FULLMASK, isnew);
     if (isnew) {
       const unsigned pos = qlen + (unsigned)__popc(nm & lanemask_lt());
@@ -609,9 +657,14 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     i += k;
 #ifdef VF_FINE_PROFILE
     W.n_rounds += 1;
+    W.f_bexp += clock64() - b1;
 #endif
     __syncwarp();
   }
+  // leave the bitmap all zero for the next search
+  __syncwarp();
+  for (unsigned t = lane; t < ntouch; t += 32u) S.vb[S.vtl[t]] = 0u;
+  __syncwarp();
   W.bfs_visits += i;
   return got;
 }

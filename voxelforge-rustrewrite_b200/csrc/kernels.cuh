@@ -136,6 +136,8 @@ struct TickSmem {
   unsigned sred[2 * 256 + 64];
   int4 pq[PRESS_QCAP];
   unsigned long long vis[VIS_CAP];
+  unsigned vb[VB_WORDS];        // pressure-search visited bitmap (zero between searches)
+  unsigned vtl[PRESS_QCAP];     // bitmap words touched by the current search
   int ring[3 * 16 * 16];
   CD pf[PF_RING][7];            // prefetched footprints (self, below, up, +x, -x, +z, -z)
   unsigned pf_ready[PF_RING];   // the cell index whose footprint a slot holds
@@ -172,7 +174,7 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.gc = nullptr;
   W.t_wait = W.t_pull = W.t_act = W.t_write = W.t_top = W.t_pc = W.t_tail = 0;
 #ifdef VF_FINE_PROFILE
-  W.f_pre = W.f_plan = W.f_seed = W.n_pc = W.n_quiet = W.n_rounds = 0;
+  W.f_pre = W.f_plan = W.f_seed = W.n_pc = W.n_quiet = W.n_rounds = W.f_bload = W.f_bexp = W.f_match = W.f_vis = 0;
 #endif
 }
 
@@ -375,7 +377,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     WS W = sW;
     W.fwd = sm.fwd;
     W.gc = sm.gc;
-    Smem S{sm.vis, ring, sm.pq};
+    Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
     const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
@@ -473,7 +475,11 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       c.prof[19] += W.n_pc;
       c.prof[20] += W.n_quiet;
       c.prof[21] += W.n_rounds;
-      sW.f_pre = sW.f_plan = sW.f_seed = sW.n_pc = sW.n_quiet = sW.n_rounds = 0;
+      c.prof[22] += W.f_bload;
+      c.prof[23] += W.f_bexp;
+      c.prof[24] += W.f_match;
+      c.prof[25] += W.f_vis;
+      sW.f_pre = sW.f_plan = sW.f_seed = sW.n_pc = sW.n_quiet = sW.n_rounds = sW.f_bload = sW.f_bexp = sW.f_match = sW.f_vis = 0;
 #endif
     }
     __syncwarp();
@@ -535,6 +541,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     ring = sm.ring;
   }
   for (unsigned i = tid; i < VIS_CAP; i += TICK_THREADS) sm.vis[i] = 0ull;
+  for (unsigned i = tid; i < VB_WORDS; i += TICK_THREADS) sm.vb[i] = 0u;
   __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds;
   __shared__ unsigned long long s_qtail;
   __shared__ WS sW;
@@ -615,7 +622,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      Smem S{sm.vis, ring, sm.pq};
+      Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl};
       W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
