@@ -149,7 +149,8 @@ int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* out);
 int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap, uint64_t* n);
 /* FluidSim::shift (src/fluid.rs:696-720): floating origin moved by (dx, dz) voxels. */
 int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz);
-/* FluidSim::reset (src/fluid.rs:318-320): the fluid state only; the world mirror stays. */
+/* FluidSim::reset (src/fluid.rs:318-320): the fluid state only; the world mirror stays, and so
+ * do the cumulative counters of vf_fluid_get_stats and vf_fluid_profile. */
 int vf_fluid_reset(vf_fluid* h);
 
 /* Differential-test snapshot: the FIFO (x,y,z triples, oldest first) and the level seed list

@@ -62,7 +62,23 @@ def assert_same_state(sim, o, box, tick=None):
     assert np.array_equal(gs, os_), f"level seeds differ{where}: {len(gs)} vs {len(os_)}"
 
 
+def assert_same_counters(sim, o, tick=None):
+    """The scheduler's counters agree too: drained cells, pull attempts (the 4096 budget), pulls
+    that took water, pressure-search queue entries examined (the 512 budget) and level cells."""
+    g, s = sim.stats(), o.stats()
+    pairs = {
+        "cell-steps": (g.cells_total, s["cells"]),
+        "pull attempts": (g.pull_attempts, s["pull_attempts"]),
+        "pull successes": (g.pull_success, s["pull_success"]),
+        "search entries": (g.bfs_visits, s["bfs_visits"]),
+        "level cells": (g.level_cells_total, s["level_cells"]),
+    }
+    bad = {k: v for k, v in pairs.items() if v[0] != v[1]}
+    assert not bad, f"counters differ after tick {tick} (gpu, oracle): {bad}"
+
+
 def assert_same_digest(sim, o, tick=None):
     g = sim.digest()
     d = o.digest()
     assert g == d, f"digest (state, fifo, seeds) differs after tick {tick}: gpu {g} oracle {d}"
+    assert_same_counters(sim, o, tick)

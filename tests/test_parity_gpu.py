@@ -292,3 +292,31 @@ def test_download_changes_in_small_batches(vf, orc):
     om, _ = o.export_box(0, 0, 0, 64, 64, 64)
     hm = np.array([[[w.get_voxel(x, y, z) for x in range(64)] for y in range(64)] for z in range(64)], np.uint8)
     assert np.array_equal(hm, om)
+
+
+def test_deep_lake_searches_hit_their_budgets(vf, orc):
+    """A lake 56 deep drained through a hole in its floor: pressure searches from the bottom
+    exhaust the 512-entry budget and the 24 side checks at the start level before they reach the
+    surface, and the tick's 4096-pull budget binds. State and counters match every tick."""
+    w = vf.World(48, 72, 48)
+    w.fill_box(0, 0, 0, 47, 3, 47, 3)          # stone floor
+    w.fill_box(0, 4, 0, 47, 71, 1, 3)          # walls
+    w.fill_box(0, 4, 46, 47, 71, 47, 3)
+    w.fill_box(0, 4, 0, 1, 71, 47, 3)
+    w.fill_box(46, 4, 0, 47, 71, 47, 3)
+    w.fill_box(2, 4, 2, 45, 59, 45, 5)         # water, 56 deep
+    w.fill_box(20, 0, 20, 27, 3, 27, 0)        # a drain hole through the floor
+    sim = vf.FluidSim(w)
+    o = oracle_for(orc, w)
+    for s_ in (sim, o):
+        s_.wake(0, 0, 0, 47, 71, 47)
+    most = 0
+    for t in range(40):
+        before = o.stats()["pull_attempts"]
+        sim.tick()
+        o.tick()
+        most = max(most, o.stats()["pull_attempts"] - before)
+        assert_same_digest(sim, o, t + 1)
+    st = o.stats()
+    assert most == 4096  # the per-tick pull budget bound
+    assert st["bfs_visits"] > 64 * st["pull_nonempty"] > 0  # long searches (over 100 entries on average)

@@ -695,6 +695,14 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   Ctl z{};
   z.atlas_used = c.atlas_used;
   z.nchg = c.nchg;  // voxel changes still owed to the host
+  // the cumulative counters and phase cycles are diagnostics, not fluid state: they run on
+  z.cells_total = c.cells_total;
+  z.pull_attempts = c.pull_attempts;
+  z.pull_success = c.pull_success;
+  z.bfs_visits = c.bfs_visits;
+  z.level_cells_total = c.level_cells_total;
+  z.activations = c.activations;
+  std::memcpy(z.prof, c.prof, sizeof(z.prof));
   CK(cudaMemcpyAsync(R.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
   h->acc = 0.0f;
   return sync_ctl(h);
