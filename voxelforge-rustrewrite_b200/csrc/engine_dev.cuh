@@ -388,9 +388,8 @@ __device__ void flush_acts(const Region& R, WS& W, const ActList& A) {
       }
     }
     W.nact = log_append(R, R.ev_act, R.ev_act_cap, W.nact, v, word, 10);
-    __syncwarp();
     W.t_act += fine_clock() - t0;
-    return;
+    return;  // the log is read only by the commit, after a CTA barrier
   }
   // immediate mode: expand the slots into single cells, 32 per round
   int total = 0;
@@ -430,8 +429,7 @@ __device__ __forceinline__ void seed_level(const Region& R, WS& W, int x, int y,
   unsigned id = dom_id(R, x, y, z);
   if (W.deferred) {  // the cap and the set membership are applied in order by the commit
     W.nseed = log_append(R, R.ev_seed, R.ev_seed_cap, W.nseed, lane_id() == 0, id, 11);
-    __syncwarp();
-    return;
+    return;  // the log is read only by the commit, after a CTA barrier
   }
   if (W.nseeds >= MAX_LEVEL_SEEDS) return;
   unsigned ins = 0;
