@@ -169,6 +169,9 @@ SUITE = [
 ]
 
 
+SUITE_TUNE_CANDIDATES = [{"producers": p, "depth": d, "ticks_per_launch": 4} for p in (4, 7) for d in (16, 64)]
+
+
 def oracle_script(orc, wl, r, warm, ticks):
     """Region r of the workload on the CPU oracle: warm-up, then the timed window with the same
     emitter and edit script as the GPU runs. Returns (cell-steps, seconds, state digest)."""
@@ -231,7 +234,7 @@ def suite(args):
     import __graft_entry__ as ge
 
     vf, orc = ge.load_package(), ge.load_oracle()
-    from vfwater import proposal, runner
+    from vfwater import autotune, proposal, runner
 
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
@@ -248,6 +251,12 @@ def suite(args):
             continue
         wl = vf.Workload(wid, 1.0, 1)
         row = {"suite": wid, "workload": desc, "regions": wl.regions, "warmup_ticks": warm, "ticks": ticks, "unit": UNIT}
+        # batched runs use the autotuner's knobs for many-region workloads (timed on a short window)
+        tune = None
+        if wl.regions > 1:
+            best, _ = autotune.tune(vf, wid, 1.0, torch, warmup=2, ticks=4, candidates=SUITE_TUNE_CANDIDATES)
+            tune = (best["producers"], best["depth"])
+            row["tuned"] = best
         # GPU: plain (one region per launch, one tick per launch, host waits each tick)
         sims = runner.make_sims(vf, wl, stream.cuda_stream)
         if warm:
@@ -262,7 +271,7 @@ def suite(args):
         for s_ in sims:
             s_.close()
         # GPU: batched, whole window as one CUDA graph
-        sims = runner.make_sims(vf, wl, stream.cuda_stream)
+        sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
         if warm:
             runner.run_batched(vf, wl, sims, 0, warm, torch, stream)
         bat = runner.run_batched(vf, wl, sims, warm, ticks, torch, stream)
@@ -270,7 +279,7 @@ def suite(args):
         for s_ in sims:
             s_.close()
         # GPU: batched + learned proposal
-        sims = runner.make_sims(vf, wl, stream.cuda_stream)
+        sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
         if warm:
             runner.run_batched(vf, wl, sims, 0, warm, torch, stream)
         lr = runner.run_learned(vf, wl, sims, warm, ticks, torch, stream, mlp)

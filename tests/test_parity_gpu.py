@@ -320,3 +320,48 @@ def test_deep_lake_searches_hit_their_budgets(vf, orc):
     st = o.stats()
     assert most == 4096  # the per-tick pull budget bound
     assert st["bfs_visits"] > 64 * st["pull_nonempty"] > 0  # long searches (over 100 entries on average)
+
+
+def test_tuning_knobs_never_change_results(vf, orc):
+    """Prefetch warps and prefetch distance change speed only: two extreme settings give the
+    oracle's state on a batch of regions."""
+    import torch
+
+    from vfwater import runner
+
+    wl = vf.Workload(3, 0.1, 4)
+    stream = torch.cuda.Stream()
+    digests = []
+    for tune in ((1, 1), (7, 64), (3, 16)):
+        sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
+        runner.run_batched(vf, wl, sims, 0, 12, torch, stream)
+        digests.append([s.digest() for s in sims])
+        for s in sims:
+            s.close()
+    assert digests[0] == digests[1] == digests[2]
+    oracles = []
+    for r in range(wl.regions):
+        o = oracle_for(orc, wl.world(r))
+        for b in wl.wakes(r):
+            o.wake(*map(int, b))
+        o.tick(12)
+        oracles.append(o.digest())
+    assert digests[0] == oracles
+
+
+def test_autotuner_times_candidates_and_caches_the_best(vf, tmp_path, monkeypatch):
+    import json
+
+    import torch
+
+    from vfwater import autotune
+
+    monkeypatch.setattr(autotune, "CACHE", tmp_path / "tune.json")
+    cands = [{"producers": 2, "depth": 8, "ticks_per_launch": 4}, {"producers": 7, "depth": 64, "ticks_per_launch": 4}]
+    best, table = autotune.tune(vf, 3, 0.1, torch, warmup=2, ticks=4, candidates=cands, seed=4)
+    assert best in [{k: c[k] for k in autotune.DEFAULT} for c in cands]
+    assert len(table) == 2 and all(r["cell_steps_per_s"] > 0 for r in table)
+    cache = json.loads((tmp_path / "tune.json").read_text())
+    (key, entry), = cache.items()
+    assert entry["best"] == best and key.endswith("|w3|S")
+    assert autotune.lookup(torch.cuda.get_device_name(), 3, vf.Workload(3, 0.1, 4).resident_cells) == best
