@@ -385,7 +385,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     for (unsigned r = 0; r < n; ++r) {
       const unsigned slot = r % PF_RING;
       // wait (bounded) for the footprint of cell r; every lane reads the same word
-      const long long tw = clock64();
+      const long long tw = fine_clock();
       unsigned long long spins = 0;
       while (*(volatile unsigned*)&sm.pf_ready[slot] != r) {
         if (++spins > SPIN_CAP_SLEEP) break;
@@ -399,7 +399,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
         break;
       }
       __threadfence_block();
-      W.t_wait += clock64() - tw;
+      W.t_wait += fine_clock() - tw;
       const int x = sm.pxyz[slot][0], y = sm.pxyz[slot][1], z = sm.pxyz[slot][2];
       const unsigned cid = (unsigned)sm.pxyz[slot][3];
       const unsigned c0 = sm.pf_c0[slot];
@@ -425,7 +425,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       }
       const bool stale = __any_sync(FULLMASK, touched);
       __syncwarp();
-      const long long t1 = clock64();
+      const long long t1 = fine_clock();
       W.t_top += t1 - tw;
       W.seq = r + 1u;
       if (!stale && (quiet & QUIET)) {
@@ -446,11 +446,11 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
         process_cell(R, W, S, x, y, z, x + ox, y + oy, z + oz, fp, mine);
       }
       __syncwarp();
-      const long long t2 = clock64();
+      const long long t2 = fine_clock();
       W.t_pc += t2 - t1;
       __threadfence_block();
       if (lane == 0) *(volatile unsigned*)&sm.consumed = r + 1u;
-      W.t_tail += clock64() - t2;
+      W.t_tail += fine_clock() - t2;
     }
     W.fwd = nullptr;
     W.gc = nullptr;
