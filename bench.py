@@ -129,7 +129,7 @@ def run_oracle(args, ticks_timed, warm):
 CPU_SAMPLE_TICKS = 500
 # DRAM bytes (read + write) of one k_tick launch of one dam-break tick, from an ncu capture
 # (profiles/k_tick_dambreak_full_capture.txt); compare with roofline.alg_bytes_per_step.
-TICK_DRAM_BYTES = 636928
+TICK_DRAM_BYTES = 636672
 
 
 def variants(args, vf, wl, torch, stream):
