@@ -406,10 +406,8 @@ def ours(args):
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         sim.tick(1)
-        ch = sim.download_changes()
-        for x, y, z, m in ch:
-            world.set_voxel(int(x), int(y), int(z), int(m))
-        d2h += 128 + 16 * len(ch) + 128  # control block after the tick and after the download, changes
+        n = sim.sync_world()  # download the tick's voxel changes, replay them through set_voxel
+        d2h += 128 + 16 * n + 128  # control block after the tick and after the download, changes
         h2d += 4 + 8  # the tick's control word and the download's pending count
     t1 = time.perf_counter()
     sD = sim.stats()

@@ -44,6 +44,11 @@ int vf_world_get_info(const vf_world* w, vf_world_info* out);
 /* Voxel access (sparse_volume.rs:228-326). */
 uint8_t vf_world_get_voxel(const vf_world* w, int32_t x, int32_t y, int32_t z);
 void vf_world_set_voxel(vf_world* w, int32_t x, int32_t y, int32_t z, uint8_t m);
+/* Replay n voxel changes through set_voxel, in order: the host side of FluidSim's write-back
+ * (src/fluid.rs:327-355 writes materials with SparseVolume::set_voxel). `changes` is an array of
+ * n records of 16 bytes as written by vf_fluid_download_changes (int32 x, y, z, uint8 material,
+ * 3 bytes padding). */
+void vf_world_set_voxels(vf_world* w, const void* changes, uint64_t n);
 void vf_world_fill_box(vf_world* w, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1, uint8_t m);
 void vf_world_fill_sphere(vf_world* w, float cx, float cy, float cz, float r, uint8_t m);
 void vf_world_compact(vf_world* w);

@@ -40,3 +40,21 @@ def test_no_device_fails_loudly(vf):
         assert e.code == -6
     else:
         raise AssertionError("FluidSim ran without a CUDA device")
+
+
+def test_world_set_voxels_replays_change_records_in_order(vf):
+    """The host write-back: 16-byte change records (x, y, z, material) go through set_voxel in
+    order, so a later record for the same voxel wins, and bricks materialise as needed."""
+    import ctypes as C
+
+    import numpy as np
+
+    w = vf.World(32, 32, 32)
+    recs = np.zeros((4, 4), np.int32)
+    recs[:, :3] = [[1, 2, 3], [9, 9, 9], [1, 2, 3], [31, 0, 31]]
+    recs[:, 3] = [5, 3, 0, 5]  # the third record overwrites the first
+    vf.lib().vf_world_set_voxels(w.h, recs.ctypes.data_as(C.c_void_p), len(recs))
+    assert w.get_voxel(1, 2, 3) == 0
+    assert w.get_voxel(9, 9, 9) == 3
+    assert w.get_voxel(31, 0, 31) == 5
+    assert w.get_voxel(0, 0, 0) == 0

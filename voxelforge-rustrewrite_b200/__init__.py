@@ -105,6 +105,7 @@ def lib():
         "vf_world_get_info": (C.c_int, [P, C.POINTER(WorldInfo)]),
         "vf_world_get_voxel": (C.c_uint8, [P, I32, I32, I32]),
         "vf_world_set_voxel": (None, [P, I32, I32, I32, C.c_uint8]),
+        "vf_world_set_voxels": (None, [P, P, C.c_uint64]),
         "vf_world_fill_box": (None, [P, I32, I32, I32, I32, I32, I32, C.c_uint8]),
         "vf_world_fill_sphere": (None, [P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint8]),
         "vf_world_compact": (None, [P]),
@@ -480,23 +481,29 @@ class FluidSim:
             arr[i].x, arr[i].y, arr[i].z, arr[i].m = x, y, z, m
         self._check(lib().vf_fluid_apply_voxel_edits(self.h, arr, len(edits)), "apply_voxel_edits")
 
-    def download_changes(self) -> np.ndarray:
+    def _download_raw(self):
         n = C.c_uint64()
         self._check(lib().vf_fluid_download_changes(self.h, None, 0, C.byref(n)), "changes")
         if n.value == 0:
-            return np.zeros((0, 4), np.int32)
+            return None, 0
         arr = (Voxel * n.value)()
         self._check(lib().vf_fluid_download_changes(self.h, arr, n.value, C.byref(n)), "changes")
+        return arr, n.value
+
+    def download_changes(self) -> np.ndarray:
+        arr, n = self._download_raw()
+        if not n:
+            return np.zeros((0, 4), np.int32)
         out = np.frombuffer(arr, dtype=np.int32).reshape(-1, 4).copy()
         out[:, 3] &= 0xFF
         return out
 
     def sync_world(self) -> int:
-        """Replay the fluid's voxel changes into the host world through set_voxel."""
-        ch = self.download_changes()
-        for x, y, z, m in ch:
-            self.world.set_voxel(int(x), int(y), int(z), int(m))
-        return len(ch)
+        """Replay the fluid's voxel changes into the host world through set_voxel (in C++)."""
+        arr, n = self._download_raw()
+        if n:
+            lib().vf_world_set_voxels(self.world.h, arr, n)
+        return n
 
     # ---- inspection (differential tests)
     def queue(self):

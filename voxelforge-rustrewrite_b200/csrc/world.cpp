@@ -452,6 +452,15 @@ int vf_world_get_info(const vf_world* w, vf_world_info* o) {
 
 uint8_t vf_world_get_voxel(const vf_world* w, int32_t x, int32_t y, int32_t z) { return w->w.get_voxel(x, y, z); }
 void vf_world_set_voxel(vf_world* w, int32_t x, int32_t y, int32_t z, uint8_t m) { w->w.set_voxel(x, y, z, m); }
+void vf_world_set_voxels(vf_world* w, const void* changes, uint64_t n) {
+  if (!w || !changes) return;
+  const unsigned char* p = static_cast<const unsigned char*>(changes);
+  for (uint64_t i = 0; i < n; ++i, p += 16) {
+    int32_t xyz[3];
+    std::memcpy(xyz, p, 12);
+    w->w.set_voxel(xyz[0], xyz[1], xyz[2], p[12]);
+  }
+}
 void vf_world_fill_box(vf_world* w, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1, uint8_t m) {
   w->w.fill_box(x0, y0, z0, x1, y1, z1, m);
 }
