@@ -58,3 +58,20 @@ def test_world_set_voxels_replays_change_records_in_order(vf):
     assert w.get_voxel(9, 9, 9) == 3
     assert w.get_voxel(31, 0, 31) == 5
     assert w.get_voxel(0, 0, 0) == 0
+
+
+def test_ring_paste_and_evict(vf):  # src/voxel/sparse_volume.rs:680-699 (the ring part)
+    """The host mirror's ring storage, as the reference's test drives it: a chunk pasted at
+    negative chunk coordinates is readable at its absolute position, nowhere else, and gone after
+    eviction."""
+    chunk = vf.World(128, 64, 128)
+    chunk.fill_sphere(64.0, 32.0, 64.0, 10.0, 4)
+    chunk.compact()
+    ring = vf.World.ring(4, 64)
+    ring.ring_paste(chunk, -3, 5)
+    assert ring.chunk_loaded(-3, 5)
+    assert ring.get_voxel(-3 * 128 + 64, 32, 5 * 128 + 64) == 4
+    assert ring.get_voxel(64, 32, 64) == 0
+    ring.ring_evict(-3, 5)
+    assert not ring.chunk_loaded(-3, 5)
+    assert ring.get_voxel(-3 * 128 + 64, 32, 5 * 128 + 64) == 0

@@ -365,3 +365,25 @@ def test_autotuner_times_candidates_and_caches_the_best(vf, tmp_path, monkeypatc
     (key, entry), = cache.items()
     assert entry["best"] == best and key.endswith("|w3|S")
     assert autotune.lookup(torch.cuda.get_device_name(), 3, vf.Workload(3, 0.1, 4).resident_cells) == best
+
+
+def test_ring_world_across_negative_coordinates(vf, orc):
+    """A ring world whose water straddles x = 0 (chunks -1 and 0): outside() follows the loaded
+    chunks, and pressure pulls skip start cells at negative x or z (fluid.rs:519), a quirk the
+    engine keeps. State and counters match the oracle every tick."""
+    chunk = vf.World(128, 64, 128)
+    chunk.fill_box(0, 0, 0, 127, 7, 127, 3)
+    ring = vf.World.ring(4, 64)
+    ring.ring_paste(chunk, -1, 0)
+    ring.ring_paste(chunk, 0, 0)
+    ring.fill_box(-20, 8, 40, 19, 30, 59, 5)   # a water block across x = 0
+    ring.fill_box(-3, 8, 45, 2, 12, 54, 0)     # a void at its foot, filled by pulls
+    sim = vf.FluidSim(ring)
+    o = oracle_for(orc, ring)
+    for s_ in (sim, o):
+        s_.wake(-24, 7, 36, 23, 34, 63)
+    for t in range(60):
+        sim.tick()
+        o.tick()
+        assert_same_digest(sim, o, t + 1)
+    assert o.stats()["pull_success"] > 0
