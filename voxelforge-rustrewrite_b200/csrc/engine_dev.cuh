@@ -2,10 +2,12 @@
 //
 // One warp owns one region's sweep: it walks the drained cells in the reference's sorted order,
 // so every cell sees exactly the state the sequential Rust loop would show it. Parallelism inside
-// a cell comes from the 32 lanes: the 7-cell footprint, the 6-cell pressure-BFS neighbourhoods and
-// the 12 cells of four level-fill membership tests load in one round each; activations are
-// deduplicated and appended to the FIFO in program order with ballots; bricks are materialised
-// cooperatively. Batching across regions runs one CTA per region (see engine.cu).
+// a cell comes from the 32 lanes: the 7-cell footprint, the writes into self, below and sides,
+// six pressure-search queue entries (5 neighbours each) and the 12 cells of four level-fill
+// membership tests go in one round each; activations, seeds and changed voxels are logged in
+// program order with ballots and committed by the whole CTA at the tick's end; bricks are
+// materialised cooperatively. Batching across regions runs one CTA per region (k_tick in
+// kernels.cuh).
 #pragma once
 #include "engine.cuh"
 
