@@ -75,3 +75,39 @@ def test_ring_paste_and_evict(vf):  # src/voxel/sparse_volume.rs:680-699 (the ri
     ring.ring_evict(-3, 5)
     assert not ring.chunk_loaded(-3, 5)
     assert ring.get_voxel(-3 * 128 + 64, 32, 5 * 128 + 64) == 0
+
+
+def test_world_set_get_compact(vf):  # src/voxel/sparse_volume.rs:643-658, on the product's host mirror
+    w = vf.World(32, 32, 32)
+    assert w.get_voxel(3, 4, 5) == 0
+    w.set_voxel(3, 4, 5, 7)
+    assert w.get_voxel(3, 4, 5) == 7
+    assert w.info.detailed == 1
+    w.set_voxel(3, 4, 5, 0)
+    w.compact()
+    assert w.info.detailed == 0
+    grid, _, _ = w.arrays()
+    assert grid[0] == 0
+    w.fill_box(8, 8, 8, 15, 15, 15, 3)
+    w.compact()
+    grid, _, _ = w.arrays()
+    assert grid[(1 * 4 + 1) * 4 + 1] == 3  # grid index (z * bricks_y + y) * bricks_x + x of brick (1, 1, 1)
+    assert w.get_voxel(-1, 0, 0) == 0
+
+
+def test_world_matches_oracle_storage_on_every_workload(vf, orc):
+    """The host mirror the engine uploads and the oracle's SparseVolume hold the same voxels for
+    every synthetic workload (region 0, sampled on a lattice)."""
+    import numpy as np
+
+    for wid in (1, 2, 3, 4, 5):
+        wl = vf.Workload(wid, 0.25 if wid in (2, 4) else 1.0, 1)
+        w = wl.world(0)
+        i = w.info
+        grid, bricks, ring = w.arrays()
+        o = orc.Oracle.from_arrays((i.nx, i.ny, i.nz, i.ring_w), grid, bricks, ring)
+        rng = np.random.default_rng(wid)
+        span_x = i.nx if not i.ring_w else 3 * 128
+        span_z = i.nz if not i.ring_w else 3 * 128
+        for x, y, z in zip(rng.integers(-2, span_x + 2, 4000), rng.integers(-2, i.ny + 2, 4000), rng.integers(-2, span_z + 2, 4000)):
+            assert w.get_voxel(int(x), int(y), int(z)) == o.get_voxel(int(x), int(y), int(z)), (wid, x, y, z)
