@@ -140,12 +140,35 @@ __device__ __forceinline__ void fwd_insert(WS& W, unsigned id, int x, int y, int
 
 constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
 
+// Neighbour loads done ahead of a pressure search by the prefetching warps while they wait.
+// The search writes nothing, so a neighbour loaded at any time during it is current. The search
+// publishes its queue; a helper claims up to six queued entries at a time. A claim is one CAS on
+// `state`, which packs the search's epoch (bits 40-63), the next unclaimed entry (bits 20-39)
+// and the helpers in flight (bits 0-19). The helper loads the entries' five neighbours into the
+// ring slot (entry % HRING), then tags the slot (epoch << 32 | entry). The search uses a slot only
+// when its tag names the current search and entry, and loads the cell itself otherwise, so it
+// never waits for a helper. Before a new search begins, the old one closes its state and waits
+// (bounded) until no helper is in flight, so no helper of an old search writes a slot again.
+constexpr unsigned HRING = 64;
+constexpr unsigned long long HELP_WAIT_CAP = 1ull << 23;  // bounded wait for helpers in flight
+struct SearchHelp {
+  CD nb[HRING][5];                // neighbours (up, +x, -x, +z, -z) of entry q at slot q % HRING
+  unsigned long long tag[HRING];  // epoch << 32 | q once nb[q % HRING] is complete
+  unsigned long long state;       // epoch << 40 | next entry << 20 | helpers in flight
+  unsigned qlen;                  // entries queued so far (published after they are written)
+  unsigned done;                  // entries the search has examined (their slots are free)
+};
+__host__ __device__ constexpr unsigned long long help_state(unsigned epoch, unsigned next, unsigned inflight) {
+  return ((unsigned long long)(epoch & 0xFFFFFFu) << 40) | ((unsigned long long)next << 20) | inflight;
+}
+
 struct Smem {
   unsigned long long* vis;  // VIS_CAP entries (epoch << 32 | id)
   const int* ring;
   int4* pq;                 // PRESS_QCAP queued cells: x, y, z and the volume (bits) seen when queued
   unsigned* vb;             // VB_WORDS: visited bitmap of the search box (all zero between searches)
   unsigned* vtl;            // PRESS_QCAP: bitmap words the current search set (cleared at its end)
+  SearchHelp* help;         // neighbour loads ahead of the search (null: none)
 };
 
 __device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
@@ -581,6 +604,21 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     visit(S, W.epoch, ntouch, x, y, z, ok, x + dx, y + dy, z + dz, nid);
   }
   __syncwarp();
+  const unsigned hep = W.epoch & 0xFFFFFFu;
+  if (S.help && hep <= 1u) {  // the 24-bit search epoch wrapped: no old tag may match again
+    for (unsigned t = lane; t < HRING; t += 32u) S.help->tag[t] = ~0ull;
+    __syncwarp();
+  }
+  SearchHelp* const H = hep ? S.help : nullptr;  // epoch 0 marks a closed search: run alone
+  if (H) {  // open the search to helpers (the previous one closed with none in flight)
+    if (lane == 0) {
+      *(volatile unsigned*)&H->qlen = qlen;
+      *(volatile unsigned*)&H->done = 0u;
+    }
+    __syncwarp();
+    __threadfence_block();
+    if (lane == 0) *(volatile unsigned long long*)&H->state = help_state(hep, 0u, 0u);
+  }
   const unsigned j = lane / 5u, d = lane - 5u * (lane / 5u);
   unsigned side = 0, i = 0;
   float got = 0.0f;
@@ -604,7 +642,17 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
       na = a + dx;
       nb = b + dy;
       nc = c + dz;
-      cd = load_cell_gc(R, W, S.ring, na, nb, nc);
+      bool have = false;
+      if (H) {
+        const unsigned q = i + j;
+        const unsigned long long tg = *(volatile unsigned long long*)&H->tag[q % HRING];
+        if (tg == (((unsigned long long)hep << 32) | q)) {
+          __threadfence_block();
+          cd = H->nb[q % HRING][d];
+          have = true;
+        }
+      }
+      if (!have) cd = load_cell_gc(R, W, S.ring, na, nb, nc);
     }
     // surface test of each entry on its up neighbour (fluid.rs:534-535)
     const bool win = act && d == 0u && (b + 1 >= R.ny || cd_solid(cd) || cd_volume(cd) <= 0.0f) && b > y && here > 0.0f;
@@ -655,10 +703,41 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
     }
     qlen += (unsigned)__popc(nm);
     i += k;
+    if (H) {  // the round's entries are examined and the new ones queued: publish both
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) {
+        *(volatile unsigned*)&H->qlen = qlen;
+        *(volatile unsigned*)&H->done = i;
+      }
+    }
 #ifdef VF_FINE_PROFILE
     W.n_rounds += 1;
     W.f_bexp += clock64() - b1;
 #endif
+    __syncwarp();
+  }
+  if (H) {  // close the search to new claims, then let the helpers in flight finish
+    unsigned ok2 = 1u;
+    if (lane == 0) {
+      unsigned long long st = *(volatile unsigned long long*)&H->state;
+      while (true) {  // clear the entry field: no claim can match it any more
+        const unsigned long long want = help_state(0u, 0u, (unsigned)(st & 0xFFFFFu));
+        const unsigned long long old = atomicCAS(&H->state, st, want);
+        if (old == st) break;
+        st = old;
+      }
+      unsigned long long spins = 0;
+      while ((*(volatile unsigned long long*)&H->state & 0xFFFFFull) != 0ull) {
+        if (++spins > HELP_WAIT_CAP) {
+          ok2 = 0u;
+          break;
+        }
+        __nanosleep(20);
+      }
+      if (!ok2) set_status(R, ST_TIMEOUT, 21);
+      __threadfence_block();
+    }
     __syncwarp();
   }
   // leave the bitmap all zero for the next search
@@ -667,6 +746,58 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
   __syncwarp();
   W.bfs_visits += i;
   return got;
+}
+
+// A prefetching warp with nothing to prefetch helps the running pressure search (SearchHelp).
+// Warp-collective; bounded work. Returns whether it loaded anything.
+__device__ bool help_search(const Region& R, const int* ring, SearchHelp* H, const int4* pq) {
+  const unsigned lane = lane_id();
+  unsigned c = 0, take = 0, ep = 0;
+  if (lane == 0) {
+    unsigned long long st = *(volatile unsigned long long*)&H->state;
+    for (int tries = 0; tries < 4; ++tries) {
+      ep = (unsigned)(st >> 40);
+      const unsigned next = (unsigned)((st >> 20) & 0xFFFFFu), inflight = (unsigned)(st & 0xFFFFFu);
+      if (ep == 0u) break;
+      __threadfence_block();
+      const unsigned ql = *(volatile unsigned*)&H->qlen, dn = *(volatile unsigned*)&H->done;
+      const unsigned lim = min(min(ql, dn + HRING), (unsigned)PRESSURE_SEARCH);
+      if (next < dn) {  // entries the search already passed: skip ahead
+        const unsigned long long old = atomicCAS(&H->state, st, help_state(ep, dn, inflight));
+        st = old == st ? help_state(ep, dn, inflight) : old;
+        continue;
+      }
+      if (next >= lim) break;
+      const unsigned t = min(PB, lim - next);
+      const unsigned long long want = help_state(ep, next + t, inflight + 1u);
+      const unsigned long long old = atomicCAS(&H->state, st, want);
+      if (old == st) {
+        c = next;
+        take = t;
+        break;
+      }
+      st = old;
+    }
+  }
+  take = __shfl_sync(FULLMASK, take, 0);
+  if (!take) return false;
+  c = __shfl_sync(FULLMASK, c, 0);
+  ep = __shfl_sync(FULLMASK, ep, 0);
+  __threadfence_block();
+  const unsigned j = lane / 5u, d = lane - 5u * (lane / 5u);
+  if (j < take) {
+    const int4 e = pq[c + j];
+    int dx, dy, dz;
+    dir5((int)d, dx, dy, dz);
+    H->nb[(c + j) % HRING][d] = load_cell(R, ring, e.x + dx, e.y + dy, e.z + dz);
+  }
+  __syncwarp();
+  __threadfence_block();
+  if (lane < take) *(volatile unsigned long long*)&H->tag[(c + lane) % HRING] = ((unsigned long long)ep << 32) | (c + lane);
+  __syncwarp();
+  __threadfence_block();
+  if (lane == 0) atomicAdd(&H->state, ~0ull);  // one helper fewer in flight (the field is >= 1)
+  return true;
 }
 
 // --------------------------------------------------------------------------- one cell

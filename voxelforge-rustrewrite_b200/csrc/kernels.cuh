@@ -146,6 +146,7 @@ struct TickSmem {
   unsigned pf_quiet[PF_RING];   // classify_quiet of the fetched footprint
   FwdEntry fwd[FWD_SIZE];       // the sweep's latest writes (store forwarding)
   unsigned long long gc[GCACHE];  // grid-word cache of the sweep's pressure searches
+  SearchHelp help;              // neighbour loads by idle prefetchers ahead of a search
   unsigned consumed;            // cells the sweep has finished
   unsigned abort;               // a wait gave up: every warp leaves the sweep
   unsigned scan[TICK_WARPS + 1];
@@ -377,7 +378,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     WS W = sW;
     W.fwd = sm.fwd;
     W.gc = sm.gc;
-    Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl};
+    Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl, &sm.help};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
     const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
@@ -497,7 +498,9 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
           ok = false;
           break;
         }
-        __nanosleep(200);  // yield issue slots to the sweep warp
+        // nothing to prefetch yet: load neighbours for a running pressure search, else yield
+        // issue slots to the sweep warp
+        if (!help_search(R, ring, &sm.help, sm.pq)) __nanosleep(200);
       }
       if (!ok) break;
       __threadfence_block();
@@ -542,6 +545,11 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
   }
   for (unsigned i = tid; i < VIS_CAP; i += TICK_THREADS) sm.vis[i] = 0ull;
   for (unsigned i = tid; i < VB_WORDS; i += TICK_THREADS) sm.vb[i] = 0u;
+  for (unsigned i = tid; i < HRING; i += TICK_THREADS) sm.help.tag[i] = ~0ull;
+  if (tid == 0) {
+    sm.help.state = 0ull;
+    sm.help.qlen = sm.help.done = 0u;
+  }
   __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds;
   __shared__ unsigned long long s_qtail;
   __shared__ WS sW;
@@ -622,7 +630,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl};
+      Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl, nullptr};
       W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
