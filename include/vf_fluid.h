@@ -190,9 +190,24 @@ int vf_mlp_forward(vf_mlp* m, const void* dev_x_f16, uint64_t n, float* dev_prob
 int vf_mlp_grads(vf_mlp* m, const void* dev_x_f16, const float* dev_y, uint64_t n, float* host_grads, void* stream);
 int vf_mlp_train_step(vf_mlp* m, const void* dev_x_f16, const float* dev_y, uint64_t n, float lr, float* host_loss, void* stream);
 
-/* Launch knobs of the tick (the autotuner's search space; results never depend on them):
+/* Launch knobs of the one-warp sweep (the autotuner's search space; results never depend on them):
  * warps prefetching footprints (1..7) and how many cells ahead of the sweep they run (1..64). */
 int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
+
+/* Which sweep runs FluidSim::tick's cell loop (src/fluid.rs:584-651); results never depend on it.
+ * engine 0: one warp walks the sorted cells (8 warps per region: the sweep and prefetchers).
+ * engine 1 (default): all 16 warps of the region's CTA walk rows of the sorted order at once, each
+ * cell waiting for the earlier cells it conflicts with; pressure searches read cells as of their own
+ * position; a segment whose order the schedule cannot keep is undone and replayed by one warp.
+ * gate (0..31, default 4): before a pressure search, wait for the earlier cells of its layer within
+ * this Chebyshev distance (fewer replays, later searches). spin_cap (> 0, default 2^24): iterations
+ * of a device wait before the tick gives up with VF_ERR_TIMEOUT.
+ * No reference counterpart: a device scheduling knob of this library. */
+int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap);
+
+/* Parallel-sweep counters summed over ticks: budget segments run, segments undone and replayed in
+ * sorted order, cells replayed. No reference counterpart (diagnostics). */
+int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed);
 
 /* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
  * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */

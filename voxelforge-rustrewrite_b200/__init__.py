@@ -154,6 +154,8 @@ def lib():
         "vf_fluid_batch_tick": (C.c_int, [C.POINTER(P), I32, I32]),
         "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_set_tuning": (C.c_int, [P, I32, I32]),
+        "vf_fluid_set_sweep": (C.c_int, [P, I32, I32, C.c_uint64]),
+        "vf_fluid_sweep_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vf_fluid_emit_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_float]),
         "vf_fluid_brush_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_uint8]),
         "vf_fluid_wake_async": (C.c_int, [P, I32, I32, I32, I32, I32, I32]),
@@ -376,8 +378,19 @@ class FluidSim:
         return bool(ch.value)
 
     def set_tuning(self, producers: int, depth: int):
-        """Launch knobs (prefetch warps, prefetch distance); results never depend on them."""
+        """Launch knobs of the one-warp sweep (prefetch warps, prefetch distance); results never depend on them."""
         self._check(lib().vf_fluid_set_tuning(self.h, producers, depth), "set_tuning")
+
+    def set_sweep(self, engine: int = 1, gate: int = 4, spin_cap: int = 1 << 24):
+        """Which sweep runs (0 one warp, 1 all warps of the region's CTA), the parallel sweep's pull
+        gate radius and the iteration cap of device waits; results never depend on them."""
+        self._check(lib().vf_fluid_set_sweep(self.h, engine, gate, spin_cap), "set_sweep")
+
+    def sweep_stats(self) -> dict:
+        """Parallel-sweep counters over all ticks: segments, segments replayed in order, cells replayed."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self._check(lib().vf_fluid_sweep_stats(self.h, C.byref(a), C.byref(b), C.byref(c)), "sweep_stats")
+        return {"segments": a.value, "rollbacks": b.value, "replayed": c.value}
 
     def emit_device_async(self, dev_xyz_ptr: int, n: int, amount: float):
         self._check(lib().vf_fluid_emit_device_async(self.h, C.c_void_p(dev_xyz_ptr), n, amount), "emit_device_async")

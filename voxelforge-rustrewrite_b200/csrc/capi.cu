@@ -34,7 +34,7 @@ struct vf_fluid {
   size_t scratch_bytes = 0;
   // tick launch shape
   int smem_bytes = 0;
-  Tune tune{TICK_WARPS - 1, PF_RING};
+  Tune tune{TICK_WARPS - 1, PF_RING, 1, 4, 1ull << 24};
   // wake proposal state (allocated on first use)
   int* slot_gi = nullptr;
   SlotAggr* aggr = nullptr;
@@ -53,6 +53,13 @@ struct vf_batch {
 };
 
 namespace {
+
+// The tick kernel of the handle's engine for `nreg` regions: one CTA per region.
+cudaError_t launch_tick(const Tune& t, Region* regs, int nreg, int n_ticks, int smem, cudaStream_t st) {
+  if (t.engine) k_tick_par<<<(unsigned)nreg, PAR_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
+  else k_tick<<<(unsigned)nreg, TICK_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
+  return cudaGetLastError();
+}
 
 int fail(vf_fluid* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -184,6 +191,7 @@ int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
   }
   h->smem_bytes = (int)sizeof(TickSmem);
   cudaFuncSetAttribute(k_tick, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_bytes);
+  cudaFuncSetAttribute(k_tick_par, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_bytes);
   *out = h;
   return VF_OK;
 }
@@ -294,6 +302,20 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.stamp, ncells, false))) return rc;
   if ((rc = dalloc(h, &R.last_woken, cap))) return rc;
   CK(cudaMemsetAsync(R.stamp, 0xFF, ncells * 4, h->stream));
+  // parallel sweep: per-cell records, rows, pull stamps and versions
+  if ((rc = dalloc(h, &R.rec, MAX_CELLS_PER_TICK))) return rc;
+  if ((rc = dalloc(h, &R.rowstart, MAX_CELLS_PER_TICK + 1))) return rc;
+  if ((rc = dalloc(h, &R.rowof, MAX_CELLS_PER_TICK))) return rc;
+  if ((rc = dalloc(h, &R.rowprog, MAX_CELLS_PER_TICK))) return rc;
+  if ((rc = dalloc(h, &R.pcnt, MAX_CELLS_PER_TICK + 1))) return rc;
+  if ((rc = dalloc(h, &R.zrow, (uint64_t)R.PY * R.PZ, false))) return rc;
+  CK(cudaMemsetAsync(R.zrow, 0xFF, (uint64_t)R.PY * R.PZ * 4, h->stream));
+  if ((rc = dalloc(h, &R.preader, ncells))) return rc;
+  if ((rc = dalloc(h, &R.ptbits, words))) return rc;
+  if ((rc = dalloc(h, &R.ptlist, MAX_PULLS_PER_TICK + 64))) return rc;
+  if ((rc = dalloc(h, &R.ptreg, PTREG_CAP))) return rc;
+  // the parallel sweep packs search-queue coordinates in 16 bits per axis
+  if (R.PX >= 65536 || R.PZ >= 65536 || R.PY >= 65536) h->tune.engine = 0;
   R.chg_cap = 1u << 22;
   if ((rc = dalloc(h, &R.chg, R.chg_cap, false))) return rc;
   uint64_t qcap = next_pow2(std::max<uint64_t>({h->want_queue, std::min<uint64_t>(ncells, 1ull << 22), 1ull << 16}));
@@ -398,8 +420,7 @@ int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks) {
   h->hzero[0] = 0u;
   CK(cudaMemcpyAsync(&h->R.ctl->changed, h->hzero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
   if (n_ticks > 0) {
-    k_tick<<<1, TICK_THREADS, h->smem_bytes, h->stream>>>(h->dR, 1, n_ticks, h->tune);
-    CK(cudaGetLastError());
+    CK(launch_tick(h->tune, h->dR, 1, n_ticks, h->smem_bytes, h->stream));
   }
   return VF_OK;
 }
@@ -691,6 +712,10 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   const uint64_t tiles = (uint64_t)R.TX * R.PY * R.TZ;
   CK(cudaMemsetAsync(R.marks, 0, tiles * 128 * 4, h->stream));
   CK(cudaMemsetAsync(R.mark_tflag, 0, tiles * 4, h->stream));
+  // per-tick maps a failed tick may have left set (cell positions, rows, pull-written cells)
+  CK(cudaMemsetAsync(R.stamp, 0xFF, (size_t)R.ncells * 4, h->stream));
+  CK(cudaMemsetAsync(R.zrow, 0xFF, (size_t)R.PY * R.PZ * 4, h->stream));
+  CK(cudaMemsetAsync(R.ptbits, 0, words * 4, h->stream));
   Ctl c = *h->hctl;
   Ctl z{};
   z.atlas_used = c.atlas_used;
@@ -863,7 +888,28 @@ int vf_fluid_stage_bricks(vf_fluid* h, const float* dev_prob, uint64_t nslots, f
 
 int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
   if (!h || producers < 1 || producers > TICK_WARPS - 1 || depth < 1 || depth > PF_RING) return VF_ERR_INVALID;
-  h->tune = Tune{producers, depth};
+  h->tune.producers = producers;
+  h->tune.depth = depth;
+  return VF_OK;
+}
+
+int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap) {
+  if (!h || engine < 0 || engine > 1 || gate < 0 || gate > GATE_MAX || spin_cap == 0) return VF_ERR_INVALID;
+  if (engine == 1 && h->uploaded && (h->R.PX >= 65536 || h->R.PZ >= 65536 || h->R.PY >= 65536))
+    return fail(h, VF_ERR_RANGE, "the parallel sweep needs domain sides below 65536");
+  h->tune.engine = engine;
+  h->tune.gate = gate;
+  h->tune.spin_cap = spin_cap;
+  return VF_OK;
+}
+
+int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (segments) *segments = h->hctl->par_segments;
+  if (rollbacks) *rollbacks = h->hctl->par_rollbacks;
+  if (replayed) *replayed = h->hctl->par_replayed;
   return VF_OK;
 }
 
@@ -935,8 +981,7 @@ int vf_batch_tick_async(vf_batch* b, int32_t n_ticks) {
   if (!b || n_ticks < 0) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
   if (n_ticks) {
-    k_tick<<<(unsigned)b->hs.size(), TICK_THREADS, h->smem_bytes, b->stream>>>(b->dregs, (int)b->hs.size(), n_ticks, h->tune);
-    CK(cudaGetLastError());
+    CK(launch_tick(h->tune, b->dregs, (int)b->hs.size(), n_ticks, h->smem_bytes, b->stream));
   }
   return VF_OK;
 }
@@ -966,7 +1011,7 @@ int vf_batch_capture(vf_batch* b, int32_t launches, int32_t ticks_per_launch) {
   }
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   for (int i = 0; i < launches; ++i)
-    k_tick<<<(unsigned)b->hs.size(), TICK_THREADS, h->smem_bytes, b->stream>>>(b->dregs, (int)b->hs.size(), ticks_per_launch, h->tune);
+    launch_tick(h->tune, b->dregs, (int)b->hs.size(), ticks_per_launch, h->smem_bytes, b->stream);
   cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
   if (e != cudaSuccess) return fail(h, VF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
   CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
@@ -1024,8 +1069,7 @@ int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks) {
   CK(cudaMemcpyAsync(h->scratch, regs.data(), sizeof(Region) * n, cudaMemcpyHostToDevice, h->stream));
   for (int i = 0; i < n; ++i) CK(cudaMemsetAsync(&regs[i].ctl->changed, 0, 4, h->stream));
   if (n_ticks) {
-    k_tick<<<n, TICK_THREADS, h->smem_bytes, h->stream>>>((Region*)h->scratch, n, n_ticks, h->tune);
-    CK(cudaGetLastError());
+    CK(launch_tick(h->tune, (Region*)h->scratch, n, n_ticks, h->smem_bytes, h->stream));
   }
   CK(cudaStreamSynchronize(h->stream));
   for (int i = 0; i < n; ++i) {

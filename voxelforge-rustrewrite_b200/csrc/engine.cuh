@@ -55,7 +55,11 @@ struct Ctl {
   unsigned int last_cells, last_level_cells, changed, mark_ntiles;
   int status;
   unsigned int err_info;
-  unsigned int pad[2];
+  unsigned int seg_epoch;           // parallel sweep: segments begun so far (tags versions and reads)
+  unsigned int ptn;                 // parallel sweep: cells listed in Region::ptlist this tick
+  // parallel sweep diagnostics, summed over ticks: budget segments run, segments rolled back and
+  // replayed in order by one warp, cells replayed
+  unsigned long long par_segments, par_rollbacks, par_replayed;
   // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear
@@ -66,6 +70,39 @@ struct Ctl {
 #endif
 };
 constexpr int NPROF = 16;
+
+// Per drained cell of the parallel sweep (global memory, indexed by sorted position). The old
+// footprint values serve readers that must see the state before this cell (multi-version reads)
+// and the rollback of a segment; the event fields are committed in sorted order at the tick's end.
+struct __align__(16) CellRec {
+  float opart[7];          // footprint partials when the cell started (self, below, up, +x, -x, +z, -z)
+  unsigned char omat[7];   // footprint materials when the cell started
+  unsigned char wmask;     // footprint cells the cell's flow wrote
+  unsigned char cmask;     // cells whose material changed: footprint bits 0..6, bit 7 the pull source
+  unsigned char amask;     // activation slots in program order (0 source, 1 self after the pull,
+                           // 2 below, 3..6 sides, 7 self)
+  unsigned char flags;     // RF_*
+  signed char pdelta;      // partial-entry count delta
+  unsigned src;            // pull source cell id
+  float src_opart;         // the source's partial before the pull wrote it
+  unsigned char src_omat;  // and its material
+  unsigned char pad0;
+  unsigned short entries;  // pressure-search queue entries examined
+};
+constexpr unsigned RF_ATTEMPT = 1u, RF_SUCCESS = 2u, RF_CHANGED = 4u, RF_SEED_SELF = 8u, RF_SEED_SRC = 16u, RF_SRCW = 32u;
+
+// A pull's write of its source cell, kept for readers earlier in sorted order that read the cell
+// after the write (open addressing by cell id; a slot belongs to the segment whose epoch it holds).
+struct __align__(16) PullTarget {
+  unsigned epoch;   // segment epoch owning the slot (claimed by CAS)
+  unsigned ready;   // == epoch once the fields below are written
+  unsigned id;      // source cell id
+  unsigned writer;  // sorted position of the pulling cell
+  float opart;      // the source's partial before the write
+  unsigned omat;    // the source's material before the write
+  unsigned pad[2];
+};
+constexpr unsigned PTREG_CAP = 16384;  // > 4 x the pulls one segment can make
 
 struct Region {
   // ---- geometry (voxel dims, brick dims, ring width; padded scheduler domain)
@@ -102,6 +139,17 @@ struct Region {
   unsigned int ev_act_cap, ev_seed_cap, ev_chg_cap;
   unsigned int* stamp;       // ncells: first event index per cell during a commit (0xFFFFFFFF idle)
   unsigned int* last_woken;  // atlas_cap: last tick a cell of the slot's brick was drained (0 = never)
+  // ---- parallel sweep (per tick; `stamp` doubles as the cell -> sorted position map)
+  CellRec* rec;          // MAX_CELLS_PER_TICK
+  unsigned* rowstart;    // MAX_CELLS_PER_TICK + 1: first sorted position of each row (y, z)
+  unsigned* rowof;       // MAX_CELLS_PER_TICK: row of each cell, bit 31 may attempt a pull, bit 30 solid
+  unsigned* rowprog;     // MAX_CELLS_PER_TICK: cells of the row finished
+  unsigned* pcnt;        // MAX_CELLS_PER_TICK + 1: exclusive prefix count of possible attempts
+  unsigned* zrow;        // PY * PZ: row of (y, z) this tick, NOSLOT otherwise
+  unsigned* preader;     // ncells: latest pull read (segment epoch << 16 | position + 1)
+  unsigned* ptbits;      // ncells bits: a pull wrote the cell this tick
+  unsigned* ptlist;      // MAX_PULLS_PER_TICK + 64 cells whose ptbits are set
+  PullTarget* ptreg;     // PTREG_CAP
   Ctl* ctl;
 };
 

@@ -5,21 +5,30 @@
 #include <cuda_fp16.h>
 
 #include "engine_dev.cuh"
+#include "sweep_par.cuh"
 
 namespace vfe {
 
+// blockDim-derived thread / warp counts of the running CTA
+#define NT_ ((unsigned)blockDim.x)
+#define NW_ ((unsigned)(blockDim.x >> 5))
+
+// Launch shapes: the one-warp sweep runs 8 warps per region (the sweep plus prefetchers), the
+// parallel sweep MAX_WARPS (row workers). CTA-wide helpers below use the launched block size;
+// shared arrays are sized for the larger shape.
 constexpr int TICK_THREADS = 256;
 constexpr int TICK_WARPS = TICK_THREADS / 32;
+constexpr int PAR_THREADS = MAX_WARPS * 32;
 
 // ---------------------------------------------------------------- CTA radix sort (LSD, 8 bit)
 // Stable within each warp's contiguous chunk; chunks in order -> stable overall. Sorts n unique
-// keys in place (tmp is scratch). hist: TICK_WARPS*256 u32 of shared memory.
+// keys in place (tmp is scratch). hist: NW_*256 u32 of shared memory.
 __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsigned* hist, unsigned* sred) {
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   if (n <= 1) return;
   // key range -> number of passes
   unsigned mn = 0xFFFFFFFFu, mx = 0;
-  for (unsigned i = tid; i < n; i += TICK_THREADS) {
+  for (unsigned i = tid; i < n; i += NT_) {
     unsigned k = keys[i];
     mn = min(mn, k);
     mx = max(mx, k);
@@ -30,37 +39,37 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
   }
   if (lane == 0) {
     sred[warp] = mn;
-    sred[TICK_WARPS + warp] = mx;
+    sred[NW_ + warp] = mx;
   }
   __syncthreads();
   if (tid == 0) {
     unsigned a = 0xFFFFFFFFu, b = 0;
-    for (int w = 0; w < TICK_WARPS; ++w) {
+    for (int w = 0; w < NW_; ++w) {
       a = min(a, sred[w]);
-      b = max(b, sred[TICK_WARPS + w]);
+      b = max(b, sred[NW_ + w]);
     }
-    sred[2 * TICK_WARPS] = a;
-    sred[2 * TICK_WARPS + 1] = b;
+    sred[2 * NW_] = a;
+    sred[2 * NW_ + 1] = b;
   }
   __syncthreads();
-  const unsigned kmin = sred[2 * TICK_WARPS], range = sred[2 * TICK_WARPS + 1] - kmin;
+  const unsigned kmin = sred[2 * NW_], range = sred[2 * NW_ + 1] - kmin;
   __syncthreads();
   const int bits = range ? 32 - __clz(range) : 0;
   const int passes = (bits + 7) / 8;
-  const unsigned chunk = (n + TICK_WARPS - 1) / TICK_WARPS;
+  const unsigned chunk = (n + NW_ - 1) / NW_;
   const unsigned b0 = min(n, warp * chunk), b1 = min(n, b0 + chunk);
   unsigned* src = keys;
   unsigned* dst = tmp;
   for (int p = 0; p < passes; ++p) {
     const int sh = 8 * p;
-    for (unsigned i = tid; i < TICK_WARPS * 256; i += TICK_THREADS) hist[i] = 0;
+    for (unsigned i = tid; i < NW_ * 256; i += NT_) hist[i] = 0;
     __syncthreads();
     for (unsigned i = b0 + lane; i < b1; i += 32) atomicAdd(&hist[warp * 256 + (((src[i] - kmin) >> sh) & 255u)], 1u);
     __syncthreads();
     // offsets: digit-major, warp-minor
     if (tid < 256) {
       unsigned s = 0;
-      for (int w = 0; w < TICK_WARPS; ++w) s += hist[w * 256 + tid];
+      for (int w = 0; w < NW_; ++w) s += hist[w * 256 + tid];
       sred[tid] = s;
     }
     __syncthreads();
@@ -85,7 +94,7 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
     __syncthreads();
     if (tid < 256) {
       unsigned run = sred[256 + tid];
-      for (int w = 0; w < TICK_WARPS; ++w) {
+      for (int w = 0; w < NW_; ++w) {
         unsigned c = hist[w * 256 + tid];
         hist[w * 256 + tid] = run;
         run += c;
@@ -114,7 +123,7 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
     dst = t;
   }
   if (src != keys) {
-    for (unsigned i = tid; i < n; i += TICK_THREADS) keys[i] = src[i];
+    for (unsigned i = tid; i < n; i += NT_) keys[i] = src[i];
     __syncthreads();
   }
 }
@@ -122,23 +131,25 @@ __device__ void cta_radix_sort(unsigned* keys, unsigned* tmp, unsigned n, unsign
 // ----------------------------------------------------------------------------- the tick
 constexpr int PF_RING = 64;                      // prefetched footprints in flight
 
-// Launch-time knobs of the tick (chosen by the autotuner; results do not depend on them):
-// producer warps prefetching footprints and how far ahead of the sweep they may run.
+// Launch-time knobs of the tick (results do not depend on them): which sweep runs, the one-warp
+// sweep's producer warps and prefetch distance (chosen by the autotuner), the parallel sweep's
+// pull gate radius and the iteration cap of device waits.
 struct Tune {
-  int producers;  // 1 .. TICK_WARPS-1
-  int depth;      // 1 .. PF_RING
+  int producers;  // one-warp sweep: 1 .. TICK_WARPS-1 prefetching warps
+  int depth;      // one-warp sweep: 1 .. PF_RING cells ahead
+  int engine;     // 0 one-warp sweep (TICK_THREADS per region), 1 parallel sweep (PAR_THREADS)
+  int gate;       // parallel sweep: 0 .. GATE_MAX
+  unsigned long long spin_cap;  // iterations before a wait gives up (ST_TIMEOUT)
 };
 constexpr unsigned long long SPIN_CAP = 1ull << 24; // bounded waits (~seconds), then an error status
 constexpr unsigned long long SPIN_CAP_SLEEP = 1ull << 23;  // waits with a nanosleep per round
 
-struct TickSmem {
-  unsigned hist[TICK_WARPS * 256];
-  unsigned sred[2 * 256 + 64];
+// Shared memory of the one-warp sweep: prefetch ring, store forwarding and search structures.
+struct SeqSmem {
   int4 pq[PRESS_QCAP];
   unsigned long long vis[VIS_CAP];
   unsigned vb[VB_WORDS];        // pressure-search visited bitmap (zero between searches)
   unsigned vtl[PRESS_QCAP];     // bitmap words touched by the current search
-  int ring[3 * 16 * 16];
   CD pf[PF_RING][7];            // prefetched footprints (self, below, up, +x, -x, +z, -z)
   unsigned pf_ready[PF_RING];   // the cell index whose footprint a slot holds
   int pxyz[PF_RING][4];         // the cell's coordinates and domain id
@@ -149,7 +160,17 @@ struct TickSmem {
   SearchHelp help;              // neighbour loads by idle prefetchers ahead of a search
   unsigned consumed;            // cells the sweep has finished
   unsigned abort;               // a wait gave up: every warp leaves the sweep
-  unsigned scan[TICK_WARPS + 1];
+};
+
+struct TickSmem {
+  unsigned hist[MAX_WARPS * 256];
+  unsigned sred[2 * 256 + 64];
+  int ring[3 * 16 * 16];
+  unsigned scan[MAX_WARPS + 1];
+  union {
+    SeqSmem s;  // one-warp sweep
+    ParSmem p;  // parallel sweep
+  } u;
 };
 
 __device__ void load_ws(const Region& R, WS& W) {
@@ -212,7 +233,7 @@ __device__ unsigned cta_scan(TickSmem& sm, bool f, unsigned* total) {
   if (lane == 0) sm.scan[warp] = __popc(b);
   __syncthreads();
   unsigned before = 0, all = 0;
-  for (int w = 0; w < TICK_WARPS; ++w) {
+  for (int w = 0; w < NW_; ++w) {
     unsigned c = sm.scan[w];
     if ((unsigned)w < warp) before += c;
     all += c;
@@ -224,12 +245,12 @@ __device__ unsigned cta_scan(TickSmem& sm, bool f, unsigned* total) {
 
 // First occurrence of each cell id in an event log (stamp = lowest event index).
 __device__ void stamp_first(const Region& R, const unsigned* ev, unsigned n) {
-  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) atomicMin(&R.stamp[ev[i]], i);
+  for (unsigned i = threadIdx.x; i < n; i += NT_) atomicMin(&R.stamp[ev[i]], i);
   __syncthreads();
 }
 __device__ void stamp_clear(const Region& R, const unsigned* ev, unsigned n) {
   __syncthreads();
-  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) R.stamp[ev[i]] = 0xFFFFFFFFu;
+  for (unsigned i = threadIdx.x; i < n; i += NT_) R.stamp[ev[i]] = 0xFFFFFFFFu;
   __syncthreads();
 }
 
@@ -246,7 +267,7 @@ __device__ unsigned cta_scan_count(TickSmem& sm, unsigned c, unsigned* total) {
   if (lane == 31) sm.scan[warp] = incl;
   __syncthreads();
   unsigned before = 0, all = 0;
-  for (int w = 0; w < TICK_WARPS; ++w) {
+  for (int w = 0; w < NW_; ++w) {
     unsigned s = sm.scan[w];
     if ((unsigned)w < warp) before += s;
     all += s;
@@ -280,7 +301,7 @@ __device__ __forceinline__ bool act_cell(const Region& R, unsigned word, int o, 
 // FIFO at its first activation if it was not active already. Log word i covers activation
 // indices 8i..8i+6, which keeps program order for the first-occurrence stamps.
 __device__ void commit_acts(const Region& R, TickSmem& sm, unsigned n, unsigned long long& qtail, unsigned long long qhead) {
-  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) {
+  for (unsigned i = threadIdx.x; i < n; i += NT_) {
     unsigned w = R.ev_act[i], id;
     for (int o = 0; o < 7; ++o)
       if (act_cell(R, w, o, id)) atomicMin(&R.stamp[id], i * 8u + (unsigned)o);
@@ -289,7 +310,7 @@ __device__ void commit_acts(const Region& R, TickSmem& sm, unsigned n, unsigned 
   __shared__ unsigned long long s_tail;
   if (threadIdx.x == 0) s_tail = qtail;
   __syncthreads();
-  for (unsigned base = 0; base < n; base += TICK_THREADS) {
+  for (unsigned base = 0; base < n; base += NT_) {
     const unsigned i = base + threadIdx.x;
     unsigned newmask = 0, w = 0;
     if (i < n) {
@@ -315,7 +336,7 @@ __device__ void commit_acts(const Region& R, TickSmem& sm, unsigned n, unsigned 
   qtail = s_tail;
   if (threadIdx.x == 0 && s_tail - qhead > R.qmask + 1ull) set_status(R, ST_OOM, 12);
   __syncthreads();
-  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) {
+  for (unsigned i = threadIdx.x; i < n; i += NT_) {
     unsigned w = R.ev_act[i], id;
     for (int o = 0; o < 7; ++o)
       if (act_cell(R, w, o, id)) R.stamp[id] = 0xFFFFFFFFu;
@@ -330,7 +351,7 @@ __device__ void commit_seeds(const Region& R, TickSmem& sm, unsigned n, unsigned
   __shared__ unsigned s_ns;
   if (threadIdx.x == 0) s_ns = nseeds;
   __syncthreads();
-  for (unsigned base = 0; base < n; base += TICK_THREADS) {
+  for (unsigned base = 0; base < n; base += NT_) {
     unsigned i = base + threadIdx.x;
     bool isnew = false;
     unsigned id = 0;
@@ -355,7 +376,7 @@ __device__ void commit_seeds(const Region& R, TickSmem& sm, unsigned n, unsigned
 
 // Voxel changes for the host (order irrelevant; the host sorts and dedups its dirty list).
 __device__ void commit_chgs(const Region& R, unsigned n) {
-  for (unsigned i = threadIdx.x; i < n; i += TICK_THREADS) record_change(R, R.ev_chg[i]);
+  for (unsigned i = threadIdx.x; i < n; i += NT_) record_change(R, R.ev_chg[i]);
   __syncthreads();
 }
 
@@ -367,18 +388,18 @@ __device__ void commit_chgs(const Region& R, unsigned n) {
 __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   if (tid == 0) {
-    sm.consumed = 0;
-    sm.abort = 0;
+    sm.u.s.consumed = 0;
+    sm.u.s.abort = 0;
   }
-  for (unsigned i = tid; i < PF_RING; i += TICK_THREADS) sm.pf_ready[i] = 0xFFFFFFFFu;
-  for (unsigned i = tid; i < FWD_SIZE; i += TICK_THREADS) sm.fwd[i].meta = 0u;
-  for (unsigned i = tid; i < GCACHE; i += TICK_THREADS) sm.gc[i] = ~0ull;
+  for (unsigned i = tid; i < PF_RING; i += NT_) sm.u.s.pf_ready[i] = 0xFFFFFFFFu;
+  for (unsigned i = tid; i < FWD_SIZE; i += NT_) sm.u.s.fwd[i].meta = 0u;
+  for (unsigned i = tid; i < GCACHE; i += NT_) sm.u.s.gc[i] = ~0ull;
   __syncthreads();
   if (warp == 0) {
     WS W = sW;
-    W.fwd = sm.fwd;
-    W.gc = sm.gc;
-    Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl, &sm.help};
+    W.fwd = sm.u.s.fwd;
+    W.gc = sm.u.s.gc;
+    Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, &sm.u.s.help};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
     const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
@@ -388,30 +409,30 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       // wait (bounded) for the footprint of cell r; every lane reads the same word
       const long long tw = fine_clock();
       unsigned long long spins = 0;
-      while (*(volatile unsigned*)&sm.pf_ready[slot] != r) {
+      while (*(volatile unsigned*)&sm.u.s.pf_ready[slot] != r) {
         if (++spins > SPIN_CAP_SLEEP) break;
         __nanosleep(20);
       }
       if (spins > SPIN_CAP_SLEEP) {
         if (lane == 0) {
           set_status(R, ST_TIMEOUT, 20);
-          *(volatile unsigned*)&sm.abort = 1u;
+          *(volatile unsigned*)&sm.u.s.abort = 1u;
         }
         break;
       }
       __threadfence_block();
       W.t_wait += fine_clock() - tw;
-      const int x = sm.pxyz[slot][0], y = sm.pxyz[slot][1], z = sm.pxyz[slot][2];
-      const unsigned cid = (unsigned)sm.pxyz[slot][3];
-      const unsigned c0 = sm.pf_c0[slot];
-      const unsigned quiet = sm.pf_quiet[slot];
+      const int x = sm.u.s.pxyz[slot][0], y = sm.u.s.pxyz[slot][1], z = sm.u.s.pxyz[slot][2];
+      const unsigned cid = (unsigned)sm.u.s.pxyz[slot][3];
+      const unsigned c0 = sm.u.s.pf_c0[slot];
+      const unsigned quiet = sm.u.s.pf_quiet[slot];
       // footprint cells the sweep wrote since the fetch: from the forwarding table, or from
       // memory when another cell's write took the cell's table entry
       bool touched = false;
       if (lane < 7) {
-        CD mine = sm.pf[slot][lane];
+        CD mine = sm.u.s.pf[slot][lane];
         const int fx = x + ox, fy = y + oy, fz = z + oz;
-        const FwdEntry e = sm.fwd[fwd_index(fx, fy, fz)];
+        const FwdEntry e = sm.u.s.fwd[fwd_index(fx, fy, fz)];
         if (!mine.out && (e.meta & 0xFFFFu) > c0) {
           touched = true;
           if (e.tag == cid + oid) {
@@ -421,7 +442,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
           } else {
             mine = load_cell(R, ring, fx, fy, fz);
           }
-          sm.pf[slot][lane] = mine;
+          sm.u.s.pf[slot][lane] = mine;
         }
       }
       const bool stale = __any_sync(FULLMASK, touched);
@@ -442,15 +463,15 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       } else {
         CD fp[7];
 #pragma unroll
-        for (int j = 0; j < 7; ++j) fp[j] = sm.pf[slot][j];
-        const CD mine = lane < 7 ? sm.pf[slot][lane] : CD{0.0f, NOSLOT, 0u, 0, true};
+        for (int j = 0; j < 7; ++j) fp[j] = sm.u.s.pf[slot][j];
+        const CD mine = lane < 7 ? sm.u.s.pf[slot][lane] : CD{0.0f, NOSLOT, 0u, 0, true};
         process_cell(R, W, S, x, y, z, x + ox, y + oy, z + oz, fp, mine);
       }
       __syncwarp();
       const long long t2 = fine_clock();
       W.t_pc += t2 - t1;
       __threadfence_block();
-      if (lane == 0) *(volatile unsigned*)&sm.consumed = r + 1u;
+      if (lane == 0) *(volatile unsigned*)&sm.u.s.consumed = r + 1u;
       W.t_tail += fine_clock() - t2;
     }
     W.fwd = nullptr;
@@ -493,14 +514,14 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       unsigned long long spins = 0;
       unsigned c0;
       bool ok = true;
-      while ((c0 = *(volatile unsigned*)&sm.consumed) + depth <= r) {
-        if (*(volatile unsigned*)&sm.abort || ++spins > SPIN_CAP_SLEEP) {
+      while ((c0 = *(volatile unsigned*)&sm.u.s.consumed) + depth <= r) {
+        if (*(volatile unsigned*)&sm.u.s.abort || ++spins > SPIN_CAP_SLEEP) {
           ok = false;
           break;
         }
         // nothing to prefetch yet: load neighbours for a running pressure search, else yield
         // issue slots to the sweep warp
-        if (!help_search(R, ring, &sm.help, sm.pq)) __nanosleep(200);
+        if (!help_search(R, ring, &sm.u.s.help, sm.u.s.pq)) __nanosleep(200);
       }
       if (!ok) break;
       __threadfence_block();
@@ -510,27 +531,330 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       const unsigned s = r % PF_RING;
       if (lane < 7) {
         int fx = x + (lane == 3) - (lane == 4), fy = y - (lane == 1) + (lane == 2), fz = z + (lane == 5) - (lane == 6);
-        sm.pf[s][lane] = load_cell_acq(R, ring, fx, fy, fz);
+        sm.u.s.pf[s][lane] = load_cell_acq(R, ring, fx, fy, fz);
       } else if (lane == 7) {
-        sm.pxyz[s][0] = x;
-        sm.pxyz[s][1] = y;
-        sm.pxyz[s][2] = z;
-        sm.pxyz[s][3] = (int)cid;
-        sm.pf_c0[s] = c0;
+        sm.u.s.pxyz[s][0] = x;
+        sm.u.s.pxyz[s][1] = y;
+        sm.u.s.pxyz[s][2] = z;
+        sm.u.s.pxyz[s][3] = (int)cid;
+        sm.u.s.pf_c0[s] = c0;
       }
       __syncwarp();
       CD fq[7];
 #pragma unroll
-      for (int j = 0; j < 7; ++j) fq[j] = sm.pf[s][j];
+      for (int j = 0; j < 7; ++j) fq[j] = sm.u.s.pf[s][j];
       const unsigned q = classify_quiet(fq, x, z);
-      if (lane == 0) sm.pf_quiet[s] = q;
+      if (lane == 0) sm.u.s.pf_quiet[s] = q;
       __syncwarp();
       __threadfence_block();
-      if (lane == 0) *(volatile unsigned*)&sm.pf_ready[s] = r;
+      if (lane == 0) *(volatile unsigned*)&sm.u.s.pf_ready[s] = r;
     }
   }
   __syncthreads();
 }
+// ------------------------------------------------------------------- the parallel sweep
+// Segment end for `room` more attempts from `pos`: the largest e <= n with at most `room` cells
+// that may attempt a pull in [pos, e).
+__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room) {
+  const unsigned lim = R.pcnt[pos] + room;
+  unsigned lo = pos + 1u, hi = n;  // answer in [pos + 1, n]
+  while (lo < hi) {
+    const unsigned m = (lo + hi + 1u) >> 1;
+    if (R.pcnt[m] <= lim) lo = m;
+    else hi = m - 1u;
+  }
+  return lo;
+}
+
+// Sum of a per-thread value over the CTA (all threads call).
+__device__ unsigned long long cta_sum(TickSmem& sm, unsigned long long v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+  __shared__ unsigned long long s_part[MAX_WARPS];
+  if ((threadIdx.x & 31u) == 0) s_part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+  for (unsigned w = 0; w < NW_; ++w) t += s_part[w];
+  __syncthreads();
+  return t;
+}
+
+// The sweep of one tick by every warp of the CTA (sweep_par.cuh describes the schedule). On return
+// the tick's activation, seed and change logs hold the sweep's events in program order and sW its
+// counters, exactly as the one-warp sweep leaves them.
+__device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
+  ParSmem& ps = sm.u.p;
+  const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const float FULL = full_level();
+  // ---- positions, rows and the cells that may attempt a pull (fluid.rs:594)
+  __shared__ unsigned s_rows, s_pc;
+  if (tid == 0) {
+    s_rows = 0;
+    s_pc = 0;
+  }
+  __syncthreads();
+  for (unsigned base = 0; base < n; base += NT_) {
+    const unsigned i = base + tid;
+    const bool valid = i < n;
+    unsigned rowflag = 0, P = 0, S = 0;
+    int x = 0, y = 0, z = 0;
+    if (valid) {
+      const unsigned key = R.cells[i];
+      const unsigned cid = key_to_id(R, key, flip);
+      R.stamp[cid] = i;
+      rowflag = (i == 0u || key / (unsigned)R.PX != R.cells[i - 1u] / (unsigned)R.PX) ? 1u : 0u;
+      dom_xyz(R, cid, x, y, z);
+      const CD c = load_cell(R, ring, x, y, z);
+      S = cd_solid(c) ? 1u : 0u;
+      if (!S) {
+        // a cell attempts only below 1 - 1e-4; one full at the tick's start gets there only as a
+        // pull's source, which must be a surface cell (up solid, outside or empty)
+        const CD u = load_cell(R, ring, x, y + 1, z);
+        P = (cd_volume(c) < FULL || cd_solid(u) || cd_volume(u) <= 0.0f) ? 1u : 0u;
+      }
+    }
+    unsigned trow, tp;
+    const unsigned orow = cta_scan_count(sm, rowflag, &trow);
+    const unsigned op = cta_scan_count(sm, P, &tp);
+    const unsigned rows0 = s_rows, pc0 = s_pc;
+    if (valid) {
+      const unsigned row = rows0 + orow + rowflag - 1u;
+      R.rowof[i] = row | (P << 31) | (S << 30);
+      R.pcnt[i] = pc0 + op;
+      if (rowflag) {
+        R.rowstart[row] = i;
+        R.rowprog[row] = 0u;
+        R.zrow[(size_t)y * (unsigned)R.PZ + (unsigned)(z - R.pz0)] = row;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      s_rows += trow;
+      s_pc += tp;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    R.rowstart[s_rows] = n;
+    R.pcnt[n] = s_pc;
+    R.ctl->ptn = 0u;
+  }
+  for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
+  for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
+  __syncthreads();
+  // ---- budget segments
+  __shared__ unsigned s_pos, s_c, s_end, s_mode, s_epoch, s_go;
+  if (tid == 0) {
+    s_pos = 0;
+    s_c = 0;
+  }
+  __syncthreads();
+  const int gate = max(0, min(tune.gate, GATE_MAX));
+  while (true) {
+    if (tid == 0) {
+      const unsigned pos = s_pos;
+      s_go = pos < n ? 1u : 0u;
+      if (s_go) {
+        if (s_c >= MAX_PULLS_PER_TICK) {
+          s_end = n;
+          s_mode = PM_NOPULL;
+        } else {
+          s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c);
+          s_mode = PM_PULL;
+        }
+        unsigned ep = R.ctl->seg_epoch + 1u;
+        if ((ep & 0xFFFFu) == 0u) ep += 1u;  // epoch 0 marks free version slots and unstamped reads
+        R.ctl->seg_epoch = ep;
+        s_epoch = ep;
+        ps.next_task = R.rowof[pos] & 0x3FFFFFFFu;
+        ps.task_end = R.rowof[s_end - 1u] & 0x3FFFFFFFu;
+        ps.abort = 0u;
+        ps.viol = 0u;
+        R.ctl->par_segments += 1ull;
+      }
+    }
+    __syncthreads();
+    if (!s_go) break;
+    ParTick T;
+    T.seg_start = s_pos;
+    T.seg_end = s_end;
+    T.epoch = s_epoch;
+    T.gate = gate;
+    T.flip = flip;
+    T.spin_cap = tune.spin_cap;
+    const int mode = (int)s_mode;
+    unsigned seq_pulls = 0;
+    // ---- row workers
+    while (true) {
+      unsigned t = 0;
+      if (lane == 0) t = atomicAdd(&ps.next_task, 1u);
+      t = __shfl_sync(FULLMASK, t, 0);
+      if (t > ps.task_end) break;
+      const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
+      bool ok = true;
+      for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls);
+      if (!ok || vld(&ps.abort)) break;
+    }
+    __syncthreads();
+    if (vld((const unsigned*)&R.ctl->status) != 0u) return;  // a wait or a capacity ran out: the tick fails
+    if (ps.viol) {
+      // a conflict the schedule could not order: undo the segment and replay it in sorted order
+      if (warp == 0) {
+        rollback_segment(R, ps, ring, T.seg_start, T.seg_end, flip);
+        for (unsigned i = T.seg_start + lane; i < T.seg_end; i += 32u) atomicAnd(&ps.state[i >> 2], ~(0xFFu << ((i & 3u) * 8u)));
+        __syncwarp();
+        const unsigned r0 = R.rowof[T.seg_start] & 0x3FFFFFFFu, r1 = R.rowof[T.seg_end - 1u] & 0x3FFFFFFFu;
+        for (unsigned r = r0 + lane; r <= r1; r += 32u) {
+          const unsigned st = R.rowstart[r];
+          R.rowprog[r] = T.seg_start > st ? T.seg_start - st : 0u;
+        }
+        __syncwarp();
+        __threadfence_block();
+        unsigned sp = s_c;
+        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp);
+        if (lane == 0) {
+          R.ctl->par_rollbacks += 1ull;
+          R.ctl->par_replayed += T.seg_end - T.seg_start;
+        }
+      }
+      __syncthreads();
+      if (vld((const unsigned*)&R.ctl->status) != 0u) return;
+    }
+    // ---- attempts made in the segment (exact: every cell of it has finished)
+    unsigned long long att = 0;
+    for (unsigned i = T.seg_start + tid; i < T.seg_end; i += NT_) att += (R.rec[i].flags & RF_ATTEMPT) ? 1u : 0u;
+    att = cta_sum(sm, att);
+    if (tid == 0) {
+      s_c += (unsigned)att;
+      s_pos = T.seg_end;
+    }
+    __syncthreads();
+  }
+  // ---- per-tick maps back to idle: positions, rows, pull-written cells
+  for (unsigned i = tid; i < n; i += NT_) {
+    const unsigned key = R.cells[i];
+    const unsigned cid = key_to_id(R, key, flip);
+    R.stamp[cid] = 0xFFFFFFFFu;
+    if (i == 0u || key / (unsigned)R.PX != R.cells[i - 1u] / (unsigned)R.PX) {
+      int x, y, z;
+      dom_xyz(R, cid, x, y, z);
+      R.zrow[(size_t)y * (unsigned)R.PZ + (unsigned)(z - R.pz0)] = NOSLOT;
+    }
+  }
+  {
+    const unsigned np = min(R.ctl->ptn, MAX_PULLS_PER_TICK + 64u);
+    for (unsigned t = tid; t < np; t += NT_) {
+      const unsigned id = R.ptlist[t];
+      atomicAnd(R.ptbits + (id >> 5), ~(1u << (id & 31u)));
+    }
+  }
+  // ---- the records in sorted order -> the tick's event logs (program order) and counters
+  __shared__ unsigned s_na, s_ns, s_nc;
+  if (tid == 0) {
+    s_na = 0;
+    s_ns = 0;
+    s_nc = 0;
+  }
+  __syncthreads();
+  const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
+  const bool lr = sW.level_round;
+  unsigned long long c_att = 0, c_succ = 0, c_ent = 0, c_chg = 0, c_pd = 0;
+  for (unsigned base = 0; base < n; base += NT_) {
+    const unsigned i = base + tid;
+    unsigned am = 0, fl = 0, cm = 0, src = 0, cid = 0;
+    if (i < n) {
+      const CellRec& rc = R.rec[i];
+      am = rc.amask;
+      fl = rc.flags;
+      cm = rc.cmask;
+      src = rc.src;
+      cid = key_to_id(R, R.cells[i], flip);
+      c_att += (fl & RF_ATTEMPT) ? 1u : 0u;
+      c_succ += (fl & RF_SUCCESS) ? 1u : 0u;
+      c_ent += rc.entries;
+      c_pd += (unsigned long long)(long long)rc.pdelta;
+      c_chg |= (fl & RF_CHANGED) ? 1u : 0u;
+    }
+    const unsigned ns = lr ? 0u : (((fl & RF_SEED_SRC) ? 1u : 0u) + ((fl & RF_SEED_SELF) ? 1u : 0u));
+    unsigned ta, ts, tc;
+    const unsigned oa = cta_scan_count(sm, (unsigned)__popc(am), &ta);
+    const unsigned os = cta_scan_count(sm, ns, &ts);
+    const unsigned oc = cta_scan_count(sm, (unsigned)__popc(cm), &tc);
+    if (i < n) {
+      // activations: slot 0 the source (one cell), slots 1..7 wake_around centres
+      unsigned pa = s_na + oa;
+      for (int g = 0; g < 8; ++g) {
+        if (!((am >> g) & 1u)) continue;
+        unsigned w;
+        switch (g) {
+          case 0: w = src; break;
+          case 2: w = (cid - (unsigned)R.PX) | ACT_AROUND; break;
+          case 3: w = (cid + 1u) | ACT_AROUND; break;
+          case 4: w = (cid - 1u) | ACT_AROUND; break;
+          case 5: w = (cid + pxy) | ACT_AROUND; break;
+          case 6: w = (cid - pxy) | ACT_AROUND; break;
+          default: w = cid | ACT_AROUND; break;  // 1 and 7: the cell itself
+        }
+        if (pa < R.ev_act_cap) R.ev_act[pa] = w;
+        else set_status(R, ST_OOM, 40);
+        ++pa;
+      }
+      unsigned psd = s_ns + os;
+      if (ns) {
+        if (fl & RF_SEED_SRC) {
+          if (psd < R.ev_seed_cap) R.ev_seed[psd] = src;
+          else set_status(R, ST_OOM, 41);
+          ++psd;
+        }
+        if (fl & RF_SEED_SELF) {
+          if (psd < R.ev_seed_cap) R.ev_seed[psd] = cid;
+          else set_status(R, ST_OOM, 41);
+        }
+      }
+      unsigned pc = s_nc + oc;
+      for (int l = 0; l < 8; ++l) {
+        if (!((cm >> l) & 1u)) continue;
+        unsigned id;
+        switch (l) {
+          case 0: id = cid; break;
+          case 1: id = cid - (unsigned)R.PX; break;
+          case 2: id = cid + (unsigned)R.PX; break;
+          case 3: id = cid + 1u; break;
+          case 4: id = cid - 1u; break;
+          case 5: id = cid + pxy; break;
+          case 6: id = cid - pxy; break;
+          default: id = src; break;
+        }
+        if (pc < R.ev_chg_cap) R.ev_chg[pc] = id;
+        else set_status(R, ST_OOM, 42);
+        ++pc;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      s_na += ta;
+      s_ns += ts;
+      s_nc += tc;
+    }
+    __syncthreads();
+  }
+  c_att = cta_sum(sm, c_att);
+  c_succ = cta_sum(sm, c_succ);
+  c_ent = cta_sum(sm, c_ent);
+  c_chg = cta_sum(sm, c_chg);
+  c_pd = cta_sum(sm, c_pd);
+  if (tid == 0) {
+    sW.nact = s_na;
+    sW.nseed = s_ns;
+    sW.nchg = s_nc;
+    sW.pull_attempts = c_att;
+    sW.pull_success = c_succ;
+    sW.bfs_visits = c_ent;
+    sW.pdelta = (long long)c_pd;
+    sW.changed = c_chg != 0;
+  }
+  __syncthreads();
+}
+
 // FluidSim::tick (fluid.rs:564-657) for region R, n_ticks times. All threads of the CTA enter.
 // Per tick: drain the FIFO head and sort it (CTA), the sweep (warp 0, prefetched by the other
 // warps), the seed log's commit, levelling (warp 0), then the activation and change logs'
@@ -540,15 +864,18 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
   const unsigned tid = threadIdx.x, warp = tid >> 5;
   const int* ring = R.ring;
   if (R.ring_w && R.ring_w <= 16) {
-    for (int i = tid; i < 3 * R.ring_w * R.ring_w; i += TICK_THREADS) sm.ring[i] = R.ring[i];
+    for (int i = tid; i < 3 * R.ring_w * R.ring_w; i += NT_) sm.ring[i] = R.ring[i];
     ring = sm.ring;
   }
-  for (unsigned i = tid; i < VIS_CAP; i += TICK_THREADS) sm.vis[i] = 0ull;
-  for (unsigned i = tid; i < VB_WORDS; i += TICK_THREADS) sm.vb[i] = 0u;
-  for (unsigned i = tid; i < HRING; i += TICK_THREADS) sm.help.tag[i] = ~0ull;
-  if (tid == 0) {
-    sm.help.state = 0ull;
-    sm.help.qlen = sm.help.done = 0u;
+  const bool par = tune.engine != 0;
+  if (!par) {
+    for (unsigned i = tid; i < VIS_CAP; i += NT_) sm.u.s.vis[i] = 0ull;
+    for (unsigned i = tid; i < VB_WORDS; i += NT_) sm.u.s.vb[i] = 0u;
+    for (unsigned i = tid; i < HRING; i += NT_) sm.u.s.help.tag[i] = ~0ull;
+    if (tid == 0) {
+      sm.u.s.help.state = 0ull;
+      sm.u.s.help.qlen = sm.u.s.help.done = 0u;
+    }
   }
   __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds;
   __shared__ unsigned long long s_qtail;
@@ -584,7 +911,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     const bool flip = s_flip != 0;
     const unsigned long long qh = sW.qhead;
     const unsigned tick_now = R.ctl->tick_no;
-    for (unsigned i = tid; i < n; i += TICK_THREADS) {
+    for (unsigned i = tid; i < n; i += NT_) {
       unsigned id = R.queue[(qh + i) & R.qmask];
       atomicAnd(&R.active[id >> 5], ~(1u << (id & 31)));
       R.cells[i] = sort_key(R, id, flip);
@@ -612,9 +939,10 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     __syncthreads();
     lap(1);
     // ---- the sweep (fluid.rs:584-651)
-    sweep(R, sm, sW, ring, n, flip, tune);
+    if (par) sweep_parallel(R, sm, sW, ring, n, flip, tune);
+    else sweep(R, sm, sW, ring, n, flip, tune);
     lap(2);
-    if (sm.abort) {
+    if (par ? vld((const unsigned*)&R.ctl->status) != 0u : sm.u.s.abort != 0u) {
       if (tid == 0) s_abort = 1;
       __syncthreads();
       break;
@@ -630,7 +958,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- levelling (fluid.rs:652-655), warp 0
     if (warp == 0) {
       WS W = sW;
-      Smem S{sm.vis, ring, sm.pq, sm.vb, sm.vtl, nullptr};
+      Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, nullptr};
       W.pdelta = 0;
       unsigned clear = 0;
       if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
@@ -676,7 +1004,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     // ---- end of a levelling round: clear the marks it touched (fluid.rs:503-505)
     if (s_clear) {
       const unsigned nt = R.ctl->mark_ntiles;
-      for (unsigned k = warp; k < nt; k += TICK_WARPS) {
+      for (unsigned k = warp; k < nt; k += NW_) {
         unsigned tile = R.mark_list[k];
         for (unsigned w = lane_id(); w < 128; w += 32) R.marks[(size_t)tile * 128u + w] = 0u;
         if (lane_id() == 0) R.mark_tflag[tile] = 0u;
@@ -692,9 +1020,22 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
   }
 }
 
+// One CTA per region. k_tick runs the one-warp sweep (TICK_THREADS per CTA), k_tick_par the
+// parallel sweep (PAR_THREADS per CTA).
 __global__ void __launch_bounds__(TICK_THREADS, 1) k_tick(Region* regs, int nreg, int n_ticks, Tune tune) {
   extern __shared__ __align__(16) unsigned char smraw[];
   TickSmem& sm = *reinterpret_cast<TickSmem*>(smraw);
+  tune.engine = 0;
+  for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
+    run_ticks(regs[r], sm, n_ticks, tune);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(PAR_THREADS, 1) k_tick_par(Region* regs, int nreg, int n_ticks, Tune tune) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TickSmem& sm = *reinterpret_cast<TickSmem*>(smraw);
+  tune.engine = 1;
   for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
     run_ticks(regs[r], sm, n_ticks, tune);
     __syncthreads();
