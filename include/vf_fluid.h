@@ -206,8 +206,11 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap);
 
 /* Parallel-sweep counters summed over ticks: budget segments run, segments undone and replayed in
- * sorted order, cells replayed. No reference counterpart (diagnostics). */
-int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed);
+ * sorted order, cells replayed, and (conflicts3, 3 entries, optional) the conflicts that caused the
+ * replays: a later reader of a pull's source had started, a later pull had read the source, the
+ * source would have joined the cells that may attempt a pull. No reference counterpart
+ * (diagnostics). */
+int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3);
 
 /* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
  * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */

@@ -155,7 +155,7 @@ def lib():
         "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_set_tuning": (C.c_int, [P, I32, I32]),
         "vf_fluid_set_sweep": (C.c_int, [P, I32, I32, C.c_uint64]),
-        "vf_fluid_sweep_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vf_fluid_sweep_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vf_fluid_emit_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_float]),
         "vf_fluid_brush_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_uint8]),
         "vf_fluid_wake_async": (C.c_int, [P, I32, I32, I32, I32, I32, I32]),
@@ -389,8 +389,10 @@ class FluidSim:
     def sweep_stats(self) -> dict:
         """Parallel-sweep counters over all ticks: segments, segments replayed in order, cells replayed."""
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
-        self._check(lib().vf_fluid_sweep_stats(self.h, C.byref(a), C.byref(b), C.byref(c)), "sweep_stats")
-        return {"segments": a.value, "rollbacks": b.value, "replayed": c.value}
+        k = (C.c_uint64 * 3)()
+        self._check(lib().vf_fluid_sweep_stats(self.h, C.byref(a), C.byref(b), C.byref(c), k), "sweep_stats")
+        return {"segments": a.value, "rollbacks": b.value, "replayed": c.value,
+                "conflicts": {"reader_started": k[0], "pull_read": k[1], "new_attempter": k[2]}}
 
     def emit_device_async(self, dev_xyz_ptr: int, n: int, amount: float):
         self._check(lib().vf_fluid_emit_device_async(self.h, C.c_void_p(dev_xyz_ptr), n, amount), "emit_device_async")

@@ -314,6 +314,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.ptbits, words))) return rc;
   if ((rc = dalloc(h, &R.ptlist, MAX_PULLS_PER_TICK + 64))) return rc;
   if ((rc = dalloc(h, &R.ptreg, PTREG_CAP))) return rc;
+  if ((rc = dalloc(h, &R.pextra, (MAX_CELLS_PER_TICK + 31) / 32))) return rc;
   // the parallel sweep packs search-queue coordinates in 16 bits per axis
   if (R.PX >= 65536 || R.PZ >= 65536 || R.PY >= 65536) h->tune.engine = 0;
   R.chg_cap = 1u << 22;
@@ -727,6 +728,11 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   z.bfs_visits = c.bfs_visits;
   z.level_cells_total = c.level_cells_total;
   z.activations = c.activations;
+  z.seg_epoch = c.seg_epoch;
+  z.par_segments = c.par_segments;
+  z.par_rollbacks = c.par_rollbacks;
+  z.par_replayed = c.par_replayed;
+  std::memcpy(z.par_conflicts, c.par_conflicts, sizeof(z.par_conflicts));
   std::memcpy(z.prof, c.prof, sizeof(z.prof));
   CK(cudaMemcpyAsync(R.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
   h->acc = 0.0f;
@@ -903,13 +909,15 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
   return VF_OK;
 }
 
-int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed) {
+int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3) {
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
   if (segments) *segments = h->hctl->par_segments;
   if (rollbacks) *rollbacks = h->hctl->par_rollbacks;
   if (replayed) *replayed = h->hctl->par_replayed;
+  if (conflicts3)
+    for (int i = 0; i < 3; ++i) conflicts3[i] = h->hctl->par_conflicts[i];
   return VF_OK;
 }
 

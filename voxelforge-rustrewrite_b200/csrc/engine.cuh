@@ -60,6 +60,9 @@ struct Ctl {
   // parallel sweep diagnostics, summed over ticks: budget segments run, segments rolled back and
   // replayed in order by one warp, cells replayed
   unsigned long long par_segments, par_rollbacks, par_replayed;
+  // conflicts by kind: a later reader of a pull's source had started, a later pull had read the
+  // source, the source would join the cells that may attempt a pull
+  unsigned long long par_conflicts[4];
   // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear
@@ -150,6 +153,7 @@ struct Region {
   unsigned* ptbits;      // ncells bits: a pull wrote the cell this tick
   unsigned* ptlist;      // MAX_PULLS_PER_TICK + 64 cells whose ptbits are set
   PullTarget* ptreg;     // PTREG_CAP
+  unsigned* pextra;      // MAX_CELLS_PER_TICK bits: later cells a pull took below 1 - 1e-4 (not counted in pcnt)
   Ctl* ctl;
 };
 

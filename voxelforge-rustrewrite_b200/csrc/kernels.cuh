@@ -553,17 +553,39 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
   __syncthreads();
 }
 // ------------------------------------------------------------------- the parallel sweep
-// Segment end for `room` more attempts from `pos`: the largest e <= n with at most `room` cells
-// that may attempt a pull in [pos, e).
-__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room) {
-  const unsigned lim = R.pcnt[pos] + room;
-  unsigned lo = pos + 1u, hi = n;  // answer in [pos + 1, n]
-  while (lo < hi) {
-    const unsigned m = (lo + hi + 1u) >> 1;
-    if (R.pcnt[m] <= lim) lo = m;
-    else hi = m - 1u;
+// Cells of [a, b) that a pull took below 1 - 1e-4 although they were not counted as possible
+// attempters (one thread).
+__device__ unsigned extra_count(const Region& R, unsigned a, unsigned b) {
+  unsigned c = 0;
+  for (unsigned w = a >> 5; w <= ((b - 1u) >> 5); ++w) {
+    unsigned m = R.pextra[w];
+    if (!m) continue;
+    if (w == (a >> 5)) m &= ~0u << (a & 31u);
+    if (w == ((b - 1u) >> 5) && ((b & 31u) != 0u)) m &= (1u << (b & 31u)) - 1u;
+    c += (unsigned)__popc(m);
   }
-  return lo;
+  return c;
+}
+
+// Segment end for `room` more attempts from `pos` (one thread): the largest e <= n such that
+// [pos, e) holds at most `room` cells that may attempt a pull, counting the cells earlier pulls of
+// the tick took below full. Cell pos itself always fits (room >= 1 leaves room for it).
+__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room) {
+  unsigned e = n;
+  for (int it = 0; it < 64; ++it) {
+    const unsigned lim = R.pcnt[pos] + room;
+    unsigned lo = pos + 1u, hi = e;  // answer in [pos + 1, e]
+    while (lo < hi) {
+      const unsigned m = (lo + hi + 1u) >> 1;
+      if (R.pcnt[m] <= lim) lo = m;
+      else hi = m - 1u;
+    }
+    const unsigned x = extra_count(R, pos, lo);
+    if (R.pcnt[lo] - R.pcnt[pos] + x <= room || lo == pos + 1u) return lo;
+    room = room > x ? room - x : 1u;
+    e = lo - 1u > pos ? lo - 1u : pos + 1u;
+  }
+  return pos + 1u;
 }
 
 // Sum of a per-thread value over the CTA (all threads call).
@@ -639,6 +661,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     R.ctl->ptn = 0u;
   }
   for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
+  for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
   for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
   __syncthreads();
   // ---- budget segments

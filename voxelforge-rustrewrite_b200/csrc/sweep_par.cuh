@@ -406,20 +406,25 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
     bool bad = false;
     if (lane == 1 && jr != NOSLOT && jr < k && jr >= T.seg_start && !wait_done(R, ps, T, jr, 35)) bad = true;
     if (__any_sync(FULLMASK, bad)) return false;
+    unsigned kind = 0;
     if (lane < 7 && jr != NOSLOT && jr > k && jr < T.seg_end) {
       if (cs_block(ps.state, jr)) blk = true;
-      else bad = true;
+      else kind = 1;
     }
     if (lane == 0) {
       const unsigned v = vld(R.preader + sid);
-      if ((v >> 16) == (T.epoch & 0xFFFFu) && (v & 0xFFFFu) > k + 1u) bad = true;
-      // possible attempters: a drained source dropping below 1 - 1e-4, or the drained cell under a
-      // source that empties (it becomes a surface cell), must have been counted
-      if (jr != NOSLOT && jr > k && jr < T.seg_end && nvv < full_level() && !(R.rowof[jr] >> 31)) bad = true;
+      if ((v >> 16) == (T.epoch & 0xFFFFu) && (v & 0xFFFFu) > k + 1u) kind = 2;
+      // a drained source taken below 1 - 1e-4 attempts a pull when its turn comes: it must be
+      // among the cells counted as possible attempters (pulls take only from surface cells, so
+      // this is a cell that became a surface during the tick). In this segment that is a conflict;
+      // in a later one the cell is counted when that segment is sized.
+      if (jr != NOSLOT && jr > k && nvv < full_level() && !(R.rowof[jr] >> 31)) {
+        if (jr < T.seg_end) kind = 3;
+        else atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u));
+      }
     }
-    const unsigned jb = __shfl_sync(FULLMASK, jr, 1);
-    if (lane == 0 && nvv <= 1e-6f && jb != NOSLOT && jb > k && jb < T.seg_end && !(R.rowof[jb] >> 31) && !((R.rowof[jb] >> 30) & 1u)) bad = true;
-    if (__any_sync(FULLMASK, bad)) {
+    if (kind) atomicAdd(&R.ctl->par_conflicts[kind - 1u], 1ull);
+    if (__any_sync(FULLMASK, kind != 0u)) {
       if (blk) cs_unblock(ps.state, jr);
       __syncwarp();
       return false;
