@@ -154,6 +154,7 @@ struct Region {
   unsigned* ptlist;      // MAX_PULLS_PER_TICK + 64 cells whose ptbits are set
   PullTarget* ptreg;     // PTREG_CAP
   unsigned* pextra;      // MAX_CELLS_PER_TICK bits: later cells a pull took below 1 - 1e-4 (not counted in pcnt)
+  unsigned* rb;          // ncells: earliest writer during a segment's rollback (0xFFFFFFFF idle)
   Ctl* ctl;
 };
 

@@ -19,6 +19,8 @@ namespace vfe {
 constexpr int TICK_THREADS = 256;
 constexpr int TICK_WARPS = TICK_THREADS / 32;
 constexpr int PAR_THREADS = MAX_WARPS * 32;
+constexpr int PEXPOSE = 3;            // water cells over a full cell that pulls may empty in one tick
+constexpr unsigned PAR_MAX_SPLITS = 6;  // conflicts at one position before it runs in order
 
 // ---------------------------------------------------------------- CTA radix sort (LSD, 8 bit)
 // Stable within each warp's contiguous chunk; chunks in order -> stable overall. Sorts n unique
@@ -628,10 +630,17 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
       const CD c = load_cell(R, ring, x, y, z);
       S = cd_solid(c) ? 1u : 0u;
       if (!S) {
-        // a cell attempts only below 1 - 1e-4; one full at the tick's start gets there only as a
-        // pull's source, which must be a surface cell (up solid, outside or empty)
-        const CD u = load_cell(R, ring, x, y + 1, z);
-        P = (cd_volume(c) < FULL || cd_solid(u) || cd_volume(u) <= 0.0f) ? 1u : 0u;
+        // A cell attempts only below 1 - 1e-4. One full at the tick's start gets there only as a
+        // pull's source, which must be a surface cell (up solid, outside or empty) when the pull
+        // runs; a cell under water becomes one after pulls empty the cells above it, one pull per
+        // cell. Cells with at most PEXPOSE water cells over them are counted; a deeper exposure
+        // in one tick is caught when the pull runs (a conflict).
+        P = cd_volume(c) < FULL ? 1u : 0u;
+        for (int d = 1; d <= PEXPOSE + 1 && !P; ++d) {
+          const CD u = load_cell(R, ring, x, y + d, z);
+          if (cd_solid(u) || cd_volume(u) <= 0.0f) P = 1u;
+          else if (d == PEXPOSE + 1) break;
+        }
       }
     }
     unsigned trow, tp;
@@ -665,10 +674,12 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
   __syncthreads();
   // ---- budget segments
-  __shared__ unsigned s_pos, s_c, s_end, s_mode, s_epoch, s_go;
+  __shared__ unsigned s_pos, s_c, s_end, s_mode, s_epoch, s_go, s_cap, s_split;
   if (tid == 0) {
     s_pos = 0;
     s_c = 0;
+    s_cap = n;    // a segment split by a conflict ends here
+    s_split = 0;  // splits of the current position so far
   }
   __syncthreads();
   const int gate = max(0, min(tune.gate, GATE_MAX));
@@ -684,6 +695,9 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
           s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c);
           s_mode = PM_PULL;
         }
+        s_end = min(s_end, max(s_cap, pos + 1u));
+        // a position split too often runs its (short) segment in order on one warp
+        if (s_split >= PAR_MAX_SPLITS) s_mode = PM_SEQ;
         unsigned ep = R.ctl->seg_epoch + 1u;
         if ((ep & 0xFFFFu) == 0u) ep += 1u;  // epoch 0 marks free version slots and unstamped reads
         R.ctl->seg_epoch = ep;
@@ -692,6 +706,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         ps.task_end = R.rowof[s_end - 1u] & 0x3FFFFFFFu;
         ps.abort = 0u;
         ps.viol = 0u;
+        ps.viol_pos = 0xFFFFFFFFu;
         R.ctl->par_segments += 1ull;
       }
     }
@@ -706,41 +721,48 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     T.spin_cap = tune.spin_cap;
     const int mode = (int)s_mode;
     unsigned seq_pulls = 0;
-    // ---- row workers
-    while (true) {
-      unsigned t = 0;
-      if (lane == 0) t = atomicAdd(&ps.next_task, 1u);
-      t = __shfl_sync(FULLMASK, t, 0);
-      if (t > ps.task_end) break;
-      const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
-      bool ok = true;
-      for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls);
-      if (!ok || vld(&ps.abort)) break;
-    }
-    __syncthreads();
-    if (vld((const unsigned*)&R.ctl->status) != 0u) return;  // a wait or a capacity ran out: the tick fails
-    if (ps.viol) {
-      // a conflict the schedule could not order: undo the segment and replay it in sorted order
+    if (mode == PM_SEQ) {
+      // one warp, in sorted order, the budget counted exactly
       if (warp == 0) {
-        rollback_segment(R, ps, ring, T.seg_start, T.seg_end, flip);
-        for (unsigned i = T.seg_start + lane; i < T.seg_end; i += 32u) atomicAnd(&ps.state[i >> 2], ~(0xFFu << ((i & 3u) * 8u)));
-        __syncwarp();
-        const unsigned r0 = R.rowof[T.seg_start] & 0x3FFFFFFFu, r1 = R.rowof[T.seg_end - 1u] & 0x3FFFFFFFu;
-        for (unsigned r = r0 + lane; r <= r1; r += 32u) {
-          const unsigned st = R.rowstart[r];
-          R.rowprog[r] = T.seg_start > st ? T.seg_start - st : 0u;
-        }
-        __syncwarp();
-        __threadfence_block();
         unsigned sp = s_c;
         for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp);
-        if (lane == 0) {
-          R.ctl->par_rollbacks += 1ull;
-          R.ctl->par_replayed += T.seg_end - T.seg_start;
-        }
+        if (lane == 0) R.ctl->par_replayed += T.seg_end - T.seg_start;
       }
       __syncthreads();
       if (vld((const unsigned*)&R.ctl->status) != 0u) return;
+    } else {
+      // ---- row workers
+      while (true) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(&ps.next_task, 1u);
+        t = __shfl_sync(FULLMASK, t, 0);
+        if (t > ps.task_end) break;
+        const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
+        bool ok = true;
+        for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls);
+        if (!ok || vld(&ps.abort)) break;
+      }
+      __syncthreads();
+      if (vld((const unsigned*)&R.ctl->status) != 0u) return;  // a wait or a capacity ran out: the tick fails
+      if (ps.viol) {
+        // a conflict the schedule could not order at pull position k: undo the segment and run it
+        // again up to k + 1 (the late reader is then outside it), the rest afterwards
+        rollback_segment(R, ps, ring, T.seg_start, T.seg_end, flip);
+        for (unsigned i = T.seg_start + tid; i < T.seg_end; i += NT_) atomicAnd(&ps.state[i >> 2], ~(0xFFu << ((i & 3u) * 8u)));
+        const unsigned r0 = R.rowof[T.seg_start] & 0x3FFFFFFFu, r1 = R.rowof[T.seg_end - 1u] & 0x3FFFFFFFu;
+        for (unsigned r = r0 + tid; r <= r1; r += NT_) {
+          const unsigned st = R.rowstart[r];
+          R.rowprog[r] = T.seg_start > st ? T.seg_start - st : 0u;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          R.ctl->par_rollbacks += 1ull;
+          s_cap = min(ps.viol_pos, T.seg_end - 1u) + 1u;
+          s_split += 1u;
+        }
+        __syncthreads();
+        continue;
+      }
     }
     // ---- attempts made in the segment (exact: every cell of it has finished)
     unsigned long long att = 0;
@@ -749,6 +771,8 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     if (tid == 0) {
       s_c += (unsigned)att;
       s_pos = T.seg_end;
+      s_cap = n;
+      s_split = 0;
     }
     __syncthreads();
   }

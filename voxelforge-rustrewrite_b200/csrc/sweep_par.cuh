@@ -51,6 +51,7 @@ struct ParSmem {
   unsigned state[(MAX_CELLS_PER_TICK + 3) / 4];  // one byte per drained cell: blockers / CS_*
   PullCtx pc[MAX_WARPS];
   unsigned next_task, task_end, abort, viol;
+  unsigned viol_pos;  // smallest sorted position of a pull that met a conflict
 };
 
 // Per-segment constants, the same on every warp.
@@ -423,7 +424,10 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
         else atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u));
       }
     }
-    if (kind) atomicAdd(&R.ctl->par_conflicts[kind - 1u], 1ull);
+    if (kind) {
+      atomicAdd(&R.ctl->par_conflicts[kind - 1u], 1ull);
+      atomicMin(&ps.viol_pos, k);
+    }
     if (__any_sync(FULLMASK, kind != 0u)) {
       if (blk) cs_unblock(ps.state, jr);
       __syncwarp();
@@ -811,41 +815,62 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   return true;
 }
 
-// Undo the writes of segment [a, b) in reverse sorted order (the order each location's writes were
-// made in), from the records: footprint writes of cells that reached CS_WRITING, then pull sources.
-__device__ void rollback_segment(const Region& R, ParSmem& ps, const int* ring, unsigned a, unsigned b, bool flip) {
-  const unsigned lane = lane_id();
-  for (unsigned i = b; i-- > a;) {
-    const unsigned st = cs_get(ps.state, i);
-    if (st < CS_STARTED) continue;
-    const unsigned cid = key_to_id(R, R.cells[i], flip);
-    int x, y, z;
-    dom_xyz(R, cid, x, y, z);
-    const CellRec& rc = R.rec[i];
-    if (st >= CS_WRITING && lane < 7u && ((rc.wmask >> lane) & 1u)) {
-      int ox, oy, oz;
-      fp_off((int)lane, ox, oy, oz);
-      const CD c = load_cell(R, ring, x + ox, y + oy, z + oz);
-      if (c.slot != NOSLOT) {
-        const size_t o = (size_t)c.slot * 512u + local_index(x + ox, y + oy, z + oz);
-        R.amat[o] = rc.omat[lane];
-        R.avol[o] = rc.opart[lane];
-      }
-    }
-    __syncwarp();
-    if (lane == 0 && (rc.flags & RF_SRCW)) {
-      int sx, sy, sz;
-      dom_xyz(R, rc.src, sx, sy, sz);
-      const CD c = load_cell(R, ring, sx, sy, sz);
-      if (c.slot != NOSLOT) {
-        const size_t o = (size_t)c.slot * 512u + local_index(sx, sy, sz);
-        R.amat[o] = rc.src_omat;
-        R.avol[o] = rc.src_opart;
-      }
-    }
-    __syncwarp();
+// Location of write slot l (0..6 footprint, 7 pull source) of the cell at sorted position i; false
+// if the cell did not make that write. Valid once the cell stopped (no warp runs in the segment).
+__device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, unsigned i, unsigned cid, unsigned l, unsigned& loc) {
+  const unsigned st = cs_get(ps.state, i);
+  if (st < CS_STARTED) return false;
+  const CellRec& rc = R.rec[i];
+  if (l == 7u) {
+    if (!(rc.flags & RF_SRCW)) return false;
+    loc = rc.src;
+    return true;
   }
-  __threadfence_block();
+  if (st < CS_WRITING || !((rc.wmask >> l) & 1u)) return false;
+  const unsigned px = (unsigned)R.PX, pxy = px * (unsigned)R.PY;
+  switch (l) {
+    case 0: loc = cid; break;
+    case 1: loc = cid - px; break;
+    case 3: loc = cid + 1u; break;
+    case 4: loc = cid - 1u; break;
+    case 5: loc = cid + pxy; break;
+    default: loc = cid - pxy; break;  // 6 (slot 2, up, is never written)
+  }
+  return true;
+}
+
+// Undo the writes of segment [a, b), CTA-wide: every cell a cell of the segment wrote gets back the
+// value its earliest writer in the segment replaced (writes to one cell were made in sorted order,
+// so that value is the cell's value at the segment's start). `rb` (one word per domain cell, all
+// 0xFFFFFFFF between calls) finds the earliest writer. All threads call; no warp may be running in
+// the segment.
+__device__ void rollback_segment(const Region& R, ParSmem& ps, const int* ring, unsigned a, unsigned b, bool flip) {
+  const unsigned nt = blockDim.x;
+  for (int phase = 0; phase < 3; ++phase) {
+    for (unsigned t = threadIdx.x; t < (b - a) * 8u; t += nt) {
+      const unsigned i = a + t / 8u, l = t % 8u;
+      if (l == 2u) continue;
+      const unsigned cid = key_to_id(R, R.cells[i], flip);
+      unsigned loc;
+      if (!rb_write(R, ps, i, cid, l, loc)) continue;
+      if (phase == 0) {
+        atomicMin(R.rb + loc, i);
+      } else if (phase == 1) {
+        if (R.rb[loc] != i) continue;
+        int x, y, z;
+        dom_xyz(R, loc, x, y, z);
+        const CD c = load_cell(R, ring, x, y, z);
+        if (c.slot == NOSLOT) continue;
+        const CellRec& rc = R.rec[i];
+        const size_t o = (size_t)c.slot * 512u + local_index(x, y, z);
+        R.amat[o] = l == 7u ? rc.src_omat : rc.omat[l];
+        R.avol[o] = l == 7u ? rc.src_opart : rc.opart[l];
+      } else {
+        R.rb[loc] = 0xFFFFFFFFu;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace vfe
