@@ -560,7 +560,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
 __device__ unsigned extra_count(const Region& R, unsigned a, unsigned b) {
   unsigned c = 0;
   for (unsigned w = a >> 5; w <= ((b - 1u) >> 5); ++w) {
-    unsigned m = R.pextra[w];
+    unsigned m = __ldcg(R.pextra + w);  // set by atomics (in L2): read past L1
     if (!m) continue;
     if (w == (a >> 5)) m &= ~0u << (a & 31u);
     if (w == ((b - 1u) >> 5) && ((b & 31u) != 0u)) m &= (1u << (b & 31u)) - 1u;
@@ -707,6 +707,12 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         ps.abort = 0u;
         ps.viol = 0u;
         ps.viol_pos = 0xFFFFFFFFu;
+        {
+          const unsigned e = s_end;
+          const unsigned used = R.pcnt[e] - R.pcnt[pos] + (s_mode == PM_PULL ? extra_count(R, pos, e) : 0u);
+          const unsigned room = s_c < MAX_PULLS_PER_TICK ? MAX_PULLS_PER_TICK - s_c : 0u;
+          ps.slack = (int)room - (int)used;
+        }
         R.ctl->par_segments += 1ull;
       }
     }

@@ -52,6 +52,7 @@ struct ParSmem {
   PullCtx pc[MAX_WARPS];
   unsigned next_task, task_end, abort, viol;
   unsigned viol_pos;  // smallest sorted position of a pull that met a conflict
+  int slack;          // attempts the segment's budget still allows beyond its counted cells
 };
 
 // Per-segment constants, the same on every warp.
@@ -420,8 +421,8 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       // this is a cell that became a surface during the tick). In this segment that is a conflict;
       // in a later one the cell is counted when that segment is sized.
       if (jr != NOSLOT && jr > k && nvv < full_level() && !(R.rowof[jr] >> 31)) {
-        if (jr < T.seg_end) kind = 3;
-        else atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u));
+        if (jr >= T.seg_end) atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u));
+        else if (atomicSub(&ps.slack, 1) <= 0) kind = 3;  // no budget left for one more attempt
       }
     }
     if (kind) {
@@ -856,7 +857,7 @@ __device__ void rollback_segment(const Region& R, ParSmem& ps, const int* ring, 
       if (phase == 0) {
         atomicMin(R.rb + loc, i);
       } else if (phase == 1) {
-        if (R.rb[loc] != i) continue;
+        if (__ldcg(R.rb + loc) != i) continue;  // set by atomics (in L2): read past L1
         int x, y, z;
         dom_xyz(R, loc, x, y, z);
         const CD c = load_cell(R, ring, x, y, z);
