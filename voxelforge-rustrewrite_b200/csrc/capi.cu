@@ -315,6 +315,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.ptlist, MAX_PULLS_PER_TICK + 64))) return rc;
   if ((rc = dalloc(h, &R.ptreg, PTREG_CAP))) return rc;
   if ((rc = dalloc(h, &R.pextra, (MAX_CELLS_PER_TICK + 31) / 32))) return rc;
+  if ((rc = dalloc(h, &R.pxlist, MAX_CELLS_PER_TICK))) return rc;
   if ((rc = dalloc(h, &R.rb, ncells, false))) return rc;
   CK(cudaMemsetAsync(R.rb, 0xFF, ncells * 4, h->stream));
   // the parallel sweep packs search-queue coordinates in 16 bits per axis

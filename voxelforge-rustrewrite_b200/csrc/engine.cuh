@@ -57,6 +57,8 @@ struct Ctl {
   unsigned int err_info;
   unsigned int seg_epoch;           // parallel sweep: segments begun so far (tags versions and reads)
   unsigned int ptn;                 // parallel sweep: cells listed in Region::ptlist this tick
+  unsigned int pxn;                 // parallel sweep: positions listed in Region::pxlist this tick
+  unsigned int pad2;
   // parallel sweep diagnostics, summed over ticks: budget segments run, segments rolled back and
   // replayed in order by one warp, cells replayed
   unsigned long long par_segments, par_rollbacks, par_replayed;
@@ -154,6 +156,7 @@ struct Region {
   unsigned* ptlist;      // MAX_PULLS_PER_TICK + 64 cells whose ptbits are set
   PullTarget* ptreg;     // PTREG_CAP
   unsigned* pextra;      // MAX_CELLS_PER_TICK bits: later cells a pull took below 1 - 1e-4 (not counted in pcnt)
+  unsigned* pxlist;      // MAX_CELLS_PER_TICK: the positions whose pextra bit is set
   unsigned* rb;          // ncells: earliest writer during a segment's rollback (0xFFFFFFFF idle)
   Ctl* ctl;
 };

@@ -555,39 +555,19 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
   __syncthreads();
 }
 // ------------------------------------------------------------------- the parallel sweep
-// Cells of [a, b) that a pull took below 1 - 1e-4 although they were not counted as possible
-// attempters (one thread).
-__device__ unsigned extra_count(const Region& R, unsigned a, unsigned b) {
-  unsigned c = 0;
-  for (unsigned w = a >> 5; w <= ((b - 1u) >> 5); ++w) {
-    unsigned m = __ldcg(R.pextra + w);  // set by atomics (in L2): read past L1
-    if (!m) continue;
-    if (w == (a >> 5)) m &= ~0u << (a & 31u);
-    if (w == ((b - 1u) >> 5) && ((b & 31u) != 0u)) m &= (1u << (b & 31u)) - 1u;
-    c += (unsigned)__popc(m);
+// Segment end for `room` more attempts from `pos` (one thread): the largest e <= n with at most
+// `room` cells in [pos, e) that may attempt a pull. `extra` cells at or after pos, taken below full
+// by earlier pulls of the tick although not counted in pcnt, are charged up front.
+__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room, unsigned extra) {
+  if (extra >= room) return pos + 1u;
+  const unsigned lim = R.pcnt[pos] + room - extra;
+  unsigned lo = pos + 1u, hi = n;  // answer in [pos + 1, n]
+  while (lo < hi) {
+    const unsigned m = (lo + hi + 1u) >> 1;
+    if (R.pcnt[m] <= lim) lo = m;
+    else hi = m - 1u;
   }
-  return c;
-}
-
-// Segment end for `room` more attempts from `pos` (one thread): the largest e <= n such that
-// [pos, e) holds at most `room` cells that may attempt a pull, counting the cells earlier pulls of
-// the tick took below full. Cell pos itself always fits (room >= 1 leaves room for it).
-__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room) {
-  unsigned e = n;
-  for (int it = 0; it < 64; ++it) {
-    const unsigned lim = R.pcnt[pos] + room;
-    unsigned lo = pos + 1u, hi = e;  // answer in [pos + 1, e]
-    while (lo < hi) {
-      const unsigned m = (lo + hi + 1u) >> 1;
-      if (R.pcnt[m] <= lim) lo = m;
-      else hi = m - 1u;
-    }
-    const unsigned x = extra_count(R, pos, lo);
-    if (R.pcnt[lo] - R.pcnt[pos] + x <= room || lo == pos + 1u) return lo;
-    room = room > x ? room - x : 1u;
-    e = lo - 1u > pos ? lo - 1u : pos + 1u;
-  }
-  return pos + 1u;
+  return lo;
 }
 
 // Sum of a per-thread value over the CTA (all threads call).
@@ -671,6 +651,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   }
   for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
   for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
+  if (tid == 0) R.ctl->pxn = 0u;
   for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
   __syncthreads();
   // ---- budget segments
@@ -683,7 +664,16 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   }
   __syncthreads();
   const int gate = max(0, min(tune.gate, GATE_MAX));
+  __shared__ unsigned s_extra;
   while (true) {
+    // cells at or after the position that earlier pulls took below full (not counted in pcnt)
+    {
+      const unsigned nx = min(__ldcg(&R.ctl->pxn), MAX_CELLS_PER_TICK);
+      unsigned long long c = 0;
+      for (unsigned q = tid; q < nx; q += NT_) c += __ldcg(R.pxlist + q) >= s_pos ? 1u : 0u;
+      c = cta_sum(sm, c);
+      if (tid == 0) s_extra = (unsigned)c;
+    }
     if (tid == 0) {
       const unsigned pos = s_pos;
       s_go = pos < n ? 1u : 0u;
@@ -692,7 +682,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
           s_end = n;
           s_mode = PM_NOPULL;
         } else {
-          s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c);
+          s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c, s_extra);
           s_mode = PM_PULL;
         }
         s_end = min(s_end, max(s_cap, pos + 1u));
@@ -709,7 +699,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         ps.viol_pos = 0xFFFFFFFFu;
         {
           const unsigned e = s_end;
-          const unsigned used = R.pcnt[e] - R.pcnt[pos] + (s_mode == PM_PULL ? extra_count(R, pos, e) : 0u);
+          const unsigned used = R.pcnt[e] - R.pcnt[pos] + (s_mode == PM_PULL ? s_extra : 0u);
           const unsigned room = s_c < MAX_PULLS_PER_TICK ? MAX_PULLS_PER_TICK - s_c : 0u;
           ps.slack = (int)room - (int)used;
         }

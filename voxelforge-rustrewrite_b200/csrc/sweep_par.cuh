@@ -333,6 +333,11 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
         if (jr[q] != NOSLOT && jr[q] < k && jr[q] >= T.seg_start && !wait_done(R, ps, T, jr[q], 34)) return false;
     }
   }
+  // stamp the read before making it: an earlier pull writes, then checks the stamp, so either it
+  // sees this stamp (a conflict) or this read sees its write
+  const unsigned id = dom_id(R, a, b, c);
+  atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
+  __threadfence();
   out = load_cell_par(R, ring, a, b, c, T.spin_cap);
   __threadfence_block();
   unsigned best = NOSLOT;
@@ -352,7 +357,6 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
       bm = rc.omat[fl];
     }
   }
-  const unsigned id = dom_id(R, a, b, c);
   if ((vld(&R.ptbits[id >> 5]) >> (id & 31u)) & 1u) {
     float op = 0.0f;
     unsigned om = 0;
@@ -367,7 +371,6 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
     out.part = bp;
     out.mat = (unsigned char)bm;
   }
-  atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
   return true;
 }
 
@@ -414,15 +417,19 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       else kind = 1;
     }
     if (lane == 0) {
-      const unsigned v = vld(R.preader + sid);
-      if ((v >> 16) == (T.epoch & 0xFFFFu) && (v & 0xFFFFu) > k + 1u) kind = 2;
       // a drained source taken below 1 - 1e-4 attempts a pull when its turn comes: it must be
       // among the cells counted as possible attempters (pulls take only from surface cells, so
       // this is a cell that became a surface during the tick). In this segment that is a conflict;
       // in a later one the cell is counted when that segment is sized.
       if (jr != NOSLOT && jr > k && nvv < full_level() && !(R.rowof[jr] >> 31)) {
-        if (jr >= T.seg_end) atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u));
-        else if (atomicSub(&ps.slack, 1) <= 0) kind = 3;  // no budget left for one more attempt
+        if (jr >= T.seg_end) {
+          if (!(atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u)) & (1u << (jr & 31u)))) {
+            const unsigned q = atomicAdd(&R.ctl->pxn, 1u);
+            if (q < MAX_CELLS_PER_TICK) R.pxlist[q] = jr;
+          }
+        } else if (atomicSub(&ps.slack, 1) <= 0) {
+          kind = 3;  // no budget left for one more attempt
+        }
       }
     }
     if (kind) {
@@ -463,8 +470,20 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
     co.src = sid;
   }
   __syncwarp();
-  __threadfence_block();
+  __threadfence();
+  // a later pull that stamped its read of the source before this write saw the old value: a
+  // conflict (the write is undone with the segment: the record holds the old value)
+  bool late = false;
+  if (mode == PM_PULL && lane == 0) {
+    const unsigned v = vld(R.preader + sid);
+    if ((v >> 16) == (T.epoch & 0xFFFFu) && (v & 0xFFFFu) > k + 1u) {
+      late = true;
+      atomicAdd(&R.ctl->par_conflicts[1], 1ull);
+      atomicMin(&ps.viol_pos, k);
+    }
+  }
   if (blk) cs_unblock(ps.state, jr);
+  if (__any_sync(FULLMASK, late)) return false;
   co.cmask = __shfl_sync(FULLMASK, co.cmask, 0);
   co.flags = __shfl_sync(FULLMASK, co.flags, 0);
   co.pdelta = __shfl_sync(FULLMASK, co.pdelta, 0);
