@@ -129,9 +129,11 @@ int vf_fluid_download_changes(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t
  * take the device-wide stall an allocation may cause, and an engine that fixes every subsystem's
  * memory budget at start-up forbids allocating later; this entry point calls no cudaMalloc,
  * cudaFree or allocating library routine. It gathers through one fixed device array of
- * VF_NOALLOC_MAX_CHANGES changes that each device keeps until the process exits; cap above that
- * is rejected with VF_ERR_RANGE. The first call on a device looks the array's address up (make
- * that first call before any stream capture). Every call on a device shares the array and
+ * VF_NOALLOC_MAX_CHANGES changes that each device keeps until the process exits; with out set, cap
+ * above that is rejected with VF_ERR_RANGE (a count-only call, out = NULL, takes any cap). The first
+ * call on a device looks the array's address up with that device current, then makes the caller's
+ * current device current again (make that first call before any stream capture). Every call on a
+ * device shares the array and
  * overwrites what the last call left there, so calls whose GPU work overlaps race: serialise them.
  * Same contract as vf_fluid_download_changes otherwise: at most cap entries, *n = total pending,
  * the rest stay pending. */

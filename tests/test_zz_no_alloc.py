@@ -70,4 +70,32 @@ def test_noalloc_download_rejects_a_cap_beyond_its_buffer(vf):
     rc = _noalloc(vf)(sim.h, buf, MAXC + 1, C.byref(n))
     assert rc == VF_ERR_RANGE
     assert b"exceeds" in vf.lib().vf_fluid_last_error(sim.h)
+    # a count-only call (no output buffer) takes any cap, like the allocating entry point
+    rc = _noalloc(vf)(sim.h, None, MAXC + 1, C.byref(n))
+    assert rc == 0
     sim.close()
+
+
+def test_noalloc_download_allocates_nothing_at_its_largest_cap(vf):
+    """At cap == VF_NOALLOC_MAX_CHANGES, on a handle whose download scratch was never grown, the
+    device's free memory is the same before and after every call."""
+    import torch
+
+    wl = vf.Workload(1)
+    a, b = vf.FluidSim(wl.world(0)), vf.FluidSim(wl.world(0))
+    for sim in (a, b):
+        for box in wl.wakes(0):
+            sim.wake(*map(int, box))
+        sim.tick(30)
+    want = _drain(vf.lib().vf_fluid_download_changes, a, vf, MAXC)
+    torch.cuda.init()
+    f = _noalloc(vf)
+    f(b.h, None, 0, C.byref(C.c_uint64()))  # first call on the device: looks the array up
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    got = _drain(f, b, vf, MAXC)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    assert got == want and len(got) > 0
+    a.close()
+    b.close()

@@ -54,6 +54,19 @@ struct vf_batch {
 
 namespace {
 
+// Makes `dev` current for a scope and gives the caller back the device it had current.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    err = cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 // The tick kernel of the handle's engine for `nreg` regions: one CTA per region.
 cudaError_t launch_tick(const Tune& t, Region* regs, int nreg, int n_ticks, int smem, cudaStream_t st) {
   if (t.engine) k_tick_par<<<(unsigned)nreg, PAR_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
@@ -155,7 +168,8 @@ int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
     delete h;
     return VF_ERR_INVALID;
   }
-  if (cudaSetDevice(h->device) != cudaSuccess) {
+  DeviceScope scope(h->device);
+  if (scope.err != cudaSuccess) {
     delete h;
     return VF_ERR_NO_DEVICE;
   }
@@ -198,7 +212,7 @@ int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
 
 void vf_fluid_destroy(vf_fluid* h) {
   if (!h) return;
-  cudaSetDevice(h->device);
+  DeviceScope scope(h->device);
   free_world(h);
   if (h->hctl) cudaFreeHost(h->hctl);
   if (h->hzero) cudaFreeHost(h->hzero);
@@ -212,7 +226,8 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
                           const uint32_t* grid, const uint8_t* bricks, uint64_t nbricks, int32_t ring_w, const int32_t* ring_slots) {
   if (!h || !grid || nx <= 0 || ny <= 0 || nz <= 0 || bricks_x <= 0 || bricks_y <= 0 || bricks_z <= 0) return VF_ERR_INVALID;
   if (ring_w && (!ring_slots || (ring_w & (ring_w - 1)))) return VF_ERR_INVALID;
-  if (cudaSetDevice(h->device) != cudaSuccess) return VF_ERR_CUDA;
+  DeviceScope scope(h->device);
+  if (scope.err != cudaSuccess) return VF_ERR_CUDA;
   if (h->uploaded) return fail(h, VF_ERR_STATE, "world already uploaded: create a new handle or use apply_voxel_edits");
   Region R{};
   R.nx = nx;
@@ -519,7 +534,8 @@ int noalloc_buffer(vf_fluid* h, Voxel** out) {
   if (h->device < 0 || h->device >= NOALLOC_MAX_DEVICES) return fail(h, VF_ERR_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_ptr[h->device]) {
-    CK(cudaSetDevice(h->device));
+    DeviceScope scope(h->device);  // the caller's current device is given back on return
+    CK(scope.err);
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_changes);
     if (e != cudaSuccess || !p) return fail(h, VF_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
@@ -554,7 +570,7 @@ __global__ void k_gather_changes_tail(Region R, unsigned long long total, unsign
 int vf_fluid_download_changes_noalloc(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n) {
   int rc = check(h);
   if (rc) return rc;
-  if (cap > VF_NOALLOC_MAX_CHANGES) {
+  if (out && cap > VF_NOALLOC_MAX_CHANGES) {
     char b[160];
     snprintf(b, sizeof b, "download_changes_noalloc: cap %llu exceeds its fixed buffer of %d changes per call",
              (unsigned long long)cap, VF_NOALLOC_MAX_CHANGES);
