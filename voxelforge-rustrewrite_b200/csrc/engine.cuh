@@ -93,6 +93,8 @@ struct __align__(16) CellRec {
   unsigned char src_omat;  // and its material
   unsigned char pad0;
   unsigned short entries;  // pressure-search queue entries examined
+  unsigned tk_main;        // execution ticket of the flow's writes (segment-wide order of writes)
+  unsigned tk_src;         // execution ticket of the pull's source write
 };
 constexpr unsigned RF_ATTEMPT = 1u, RF_SUCCESS = 2u, RF_CHANGED = 4u, RF_SEED_SELF = 8u, RF_SEED_SRC = 16u, RF_SRCW = 32u;
 

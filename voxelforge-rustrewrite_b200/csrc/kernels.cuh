@@ -697,6 +697,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         ps.abort = 0u;
         ps.viol = 0u;
         ps.viol_pos = 0xFFFFFFFFu;
+        ps.ticket = 0u;
         {
           const unsigned e = s_end;
           const unsigned used = R.pcnt[e] - R.pcnt[pos] + (s_mode == PM_PULL ? s_extra : 0u);

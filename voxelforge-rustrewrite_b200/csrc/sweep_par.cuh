@@ -53,6 +53,7 @@ struct ParSmem {
   unsigned next_task, task_end, abort, viol;
   unsigned viol_pos;  // smallest sorted position of a pull that met a conflict
   int slack;          // attempts the segment's budget still allows beyond its counted cells
+  unsigned ticket;    // execution order of write groups in the segment (rollback restores the first)
 };
 
 // Per-segment constants, the same on every warp.
@@ -442,6 +443,26 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       return false;
     }
   }
+  // Pull writes of one source are made one at a time (a lock on the source's rollback word, idle
+  // during the sweep), so their tickets and recorded old values follow the order of the writes.
+  bool locked = true;
+  if (mode == PM_PULL && lane == 0) {
+    unsigned long long spins = 0;
+    while (atomicCAS(R.rb + sid, 0xFFFFFFFFu, k) != 0xFFFFFFFFu) {
+      if (++spins > T.spin_cap) {
+        par_timeout(R, ps, 43);
+        locked = false;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+  }
+  if (!__shfl_sync(FULLMASK, locked ? 1u : 0u, 0)) {
+    if (blk) cs_unblock(ps.state, jr);
+    __syncwarp();
+    return false;
+  }
   CD c = CD{0.0f, NOSLOT, 0u, 0, true};
   if (lane == 0) c = load_cell_par(R, ring, wa, wb, wc, T.spin_cap);
   const bool need = lane == 0 && c.slot == NOSLOT && set_volume_needs_slot(c, nvv);
@@ -451,6 +472,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
     rc->src = sid;
     rc->src_opart = c.part;
     rc->src_omat = c.mat;
+    rc->tk_src = atomicAdd(&ps.ticket, 1u);
     rc->flags = RF_SRCW;
     if (mode == PM_PULL) {
       ptreg_insert(R, T.epoch, sid, k, c.part, c.mat);
@@ -481,6 +503,8 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       atomicAdd(&R.ctl->par_conflicts[1], 1ull);
       atomicMin(&ps.viol_pos, k);
     }
+    __threadfence();
+    atomicExch(R.rb + sid, 0xFFFFFFFFu);
   }
   if (blk) cs_unblock(ps.state, jr);
   if (__any_sync(FULLMASK, late)) return false;
@@ -813,6 +837,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
     rc->pdelta = (signed char)co.pdelta;
     rc->src = co.src;
     rc->entries = (unsigned short)co.entries;
+    rc->tk_main = atomicAdd(&ps.ticket, 1u);
   }
   __syncwarp();
   __threadfence_block();
@@ -835,18 +860,22 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   return true;
 }
 
-// Location of write slot l (0..6 footprint, 7 pull source) of the cell at sorted position i; false
-// if the cell did not make that write. Valid once the cell stopped (no warp runs in the segment).
-__device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, unsigned i, unsigned cid, unsigned l, unsigned& loc) {
+// Location and execution ticket of write slot l (0..6 footprint, 7 pull source) of the cell at
+// sorted position i; false if the cell did not make that write. Valid once the cell stopped (no warp
+// runs in the segment).
+__device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, unsigned i, unsigned cid, unsigned l, unsigned& loc,
+                                         unsigned& tk) {
   const unsigned st = cs_get(ps.state, i);
   if (st < CS_STARTED) return false;
   const CellRec& rc = R.rec[i];
   if (l == 7u) {
     if (!(rc.flags & RF_SRCW)) return false;
     loc = rc.src;
+    tk = rc.tk_src;
     return true;
   }
   if (st < CS_WRITING || !((rc.wmask >> l) & 1u)) return false;
+  tk = rc.tk_main;
   const unsigned px = (unsigned)R.PX, pxy = px * (unsigned)R.PY;
   switch (l) {
     case 0: loc = cid; break;
@@ -859,11 +888,10 @@ __device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, uns
   return true;
 }
 
-// Undo the writes of segment [a, b), CTA-wide: every cell a cell of the segment wrote gets back the
-// value its earliest writer in the segment replaced (writes to one cell were made in sorted order,
-// so that value is the cell's value at the segment's start). `rb` (one word per domain cell, all
-// 0xFFFFFFFF between calls) finds the earliest writer. All threads call; no warp may be running in
-// the segment.
+// Undo the writes of segment [a, b), CTA-wide: every cell written in the segment gets back the
+// value replaced by its first write in execution order (tickets), which is its value at the
+// segment's start. `rb` (one word per domain cell, all 0xFFFFFFFF between calls) finds that write.
+// All threads call; no warp may be running in the segment.
 __device__ void rollback_segment(const Region& R, ParSmem& ps, const int* ring, unsigned a, unsigned b, bool flip) {
   const unsigned nt = blockDim.x;
   for (int phase = 0; phase < 3; ++phase) {
@@ -871,12 +899,12 @@ __device__ void rollback_segment(const Region& R, ParSmem& ps, const int* ring, 
       const unsigned i = a + t / 8u, l = t % 8u;
       if (l == 2u) continue;
       const unsigned cid = key_to_id(R, R.cells[i], flip);
-      unsigned loc;
-      if (!rb_write(R, ps, i, cid, l, loc)) continue;
+      unsigned loc, tk;
+      if (!rb_write(R, ps, i, cid, l, loc, tk)) continue;
       if (phase == 0) {
-        atomicMin(R.rb + loc, i);
+        atomicMin(R.rb + loc, tk);
       } else if (phase == 1) {
-        if (__ldcg(R.rb + loc) != i) continue;  // set by atomics (in L2): read past L1
+        if (__ldcg(R.rb + loc) != tk) continue;  // set by atomics (in L2): read past L1
         int x, y, z;
         dom_xyz(R, loc, x, y, z);
         const CD c = load_cell(R, ring, x, y, z);
