@@ -214,6 +214,11 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
  * (diagnostics). */
 int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3);
 
+/* Parallel-sweep SM cycle counters summed over ticks (12 entries): prepass, segments, rollbacks,
+ * event logs; then summed over warps: dependency waits, blocked starts, footprint loads, pulls,
+ * writes, cells run, row fetches, worker total. No reference counterpart (diagnostics). */
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out12);
+
 /* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
  * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */
 int vf_fluid_emit_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, float amount);

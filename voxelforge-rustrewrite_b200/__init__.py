@@ -155,6 +155,7 @@ def lib():
         "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_set_tuning": (C.c_int, [P, I32, I32]),
         "vf_fluid_set_sweep": (C.c_int, [P, I32, I32, C.c_uint64]),
+        "vf_fluid_sweep_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_sweep_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vf_fluid_emit_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_float]),
         "vf_fluid_brush_device_async": (C.c_int, [P, C.c_void_p, U64, C.c_uint8]),
@@ -385,6 +386,15 @@ class FluidSim:
         """Which sweep runs (0 one warp, 1 all warps of the region's CTA), the parallel sweep's pull
         gate radius and the iteration cap of device waits; results never depend on them."""
         self._check(lib().vf_fluid_set_sweep(self.h, engine, gate, spin_cap), "set_sweep")
+
+    SWEEP_PROFILE = ("prepass", "segments", "rollbacks", "logs", "dep_wait", "start_wait", "footprint", "pulls", "writes", "cells",
+                     "row_fetch", "worker_total")
+
+    def sweep_profile(self) -> dict:
+        """Parallel-sweep SM cycle counters summed over ticks (the per-cell ones also over warps)."""
+        a = (C.c_uint64 * 12)()
+        self._check(lib().vf_fluid_sweep_profile(self.h, a), "sweep_profile")
+        return dict(zip(self.SWEEP_PROFILE, map(int, a)))
 
     def sweep_stats(self) -> dict:
         """Parallel-sweep counters over all ticks: segments, segments replayed in order, cells replayed."""

@@ -752,6 +752,7 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   z.par_rollbacks = c.par_rollbacks;
   z.par_replayed = c.par_replayed;
   std::memcpy(z.par_conflicts, c.par_conflicts, sizeof(z.par_conflicts));
+  std::memcpy(z.pprof, c.pprof, sizeof(z.pprof));
   std::memcpy(z.prof, c.prof, sizeof(z.prof));
   CK(cudaMemcpyAsync(R.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
   h->acc = 0.0f;
@@ -925,6 +926,14 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
   h->tune.engine = engine;
   h->tune.gate = gate;
   h->tune.spin_cap = spin_cap;
+  return VF_OK;
+}
+
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out12) {
+  int rc = check(h);
+  if (rc) return rc;
+  if ((rc = sync_ctl(h))) return rc;
+  if (out12) std::memcpy(out12, h->hctl->pprof, 12 * sizeof(uint64_t));
   return VF_OK;
 }
 

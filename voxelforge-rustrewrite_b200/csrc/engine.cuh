@@ -65,6 +65,10 @@ struct Ctl {
   // conflicts by kind: a later reader of a pull's source had started, a later pull had read the
   // source, the source would join the cells that may attempt a pull
   unsigned long long par_conflicts[4];
+  // parallel sweep cycle counters: 0 prepass, 1 segments (workers), 2 rollbacks, 3 event logs;
+  // summed over warps: 4 dependency waits, 5 start (blocked), 6 footprint loads, 7 pulls (gate and
+  // search), 8 writes, 9 cells run, 10 between cells (row fetch), 11 worker total
+  unsigned long long pprof[12];
   // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear

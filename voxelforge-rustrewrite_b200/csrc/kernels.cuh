@@ -589,6 +589,16 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   ParSmem& ps = sm.u.p;
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const float FULL = full_level();
+  long long tp0 = clock64();
+  auto plap = [&](int k) {
+    if (tid == 0) {
+      const long long now = clock64();
+      R.ctl->pprof[k] += (unsigned long long)(now - tp0);
+      tp0 = now;
+    }
+  };
+  ParProf pf{0, 0, 0, 0, 0, 0};
+  unsigned long long w_fetch = 0, w_total = 0;
   // ---- positions, rows and the cells that may attempt a pull (fluid.rs:594)
   __shared__ unsigned s_rows, s_pc;
   if (tid == 0) {
@@ -654,6 +664,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   if (tid == 0) R.ctl->pxn = 0u;
   for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
   __syncthreads();
+  plap(0);
   // ---- budget segments
   __shared__ unsigned s_pos, s_c, s_end, s_mode, s_epoch, s_go, s_cap, s_split;
   if (tid == 0) {
@@ -722,24 +733,29 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
       // one warp, in sorted order, the budget counted exactly
       if (warp == 0) {
         unsigned sp = s_c;
-        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp);
+        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf);
         if (lane == 0) R.ctl->par_replayed += T.seg_end - T.seg_start;
       }
       __syncthreads();
       if (vld((const unsigned*)&R.ctl->status) != 0u) return;
     } else {
       // ---- row workers
+      const long long w0 = clock64();
       while (true) {
+        const long long f0 = clock64();
         unsigned t = 0;
         if (lane == 0) t = atomicAdd(&ps.next_task, 1u);
         t = __shfl_sync(FULLMASK, t, 0);
         if (t > ps.task_end) break;
         const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
+        w_fetch += (unsigned long long)(clock64() - f0);
         bool ok = true;
-        for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls);
+        for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf);
         if (!ok || vld(&ps.abort)) break;
       }
+      w_total += (unsigned long long)(clock64() - w0);
       __syncthreads();
+      plap(1);
       if (vld((const unsigned*)&R.ctl->status) != 0u) return;  // a wait or a capacity ran out: the tick fails
       if (ps.viol) {
         // a conflict the schedule could not order at pull position k: undo the segment and run it
@@ -752,6 +768,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
           R.rowprog[r] = T.seg_start > st ? T.seg_start - st : 0u;
         }
         __syncthreads();
+        plap(2);
         if (tid == 0) {
           R.ctl->par_rollbacks += 1ull;
           s_cap = min(ps.viol_pos, T.seg_end - 1u) + 1u;
@@ -773,6 +790,18 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     }
     __syncthreads();
   }
+  if (lane == 0) {
+    unsigned long long* q = R.ctl->pprof;
+    atomicAdd(q + 4, pf.dep);
+    atomicAdd(q + 5, pf.start);
+    atomicAdd(q + 6, pf.load);
+    atomicAdd(q + 7, pf.pull);
+    atomicAdd(q + 8, pf.write);
+    atomicAdd(q + 9, pf.cells);
+    atomicAdd(q + 10, w_fetch);
+    atomicAdd(q + 11, w_total);
+  }
+  tp0 = clock64();
   // ---- per-tick maps back to idle: positions, rows, pull-written cells
   for (unsigned i = tid; i < n; i += NT_) {
     const unsigned key = R.cells[i];
@@ -897,6 +926,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     sW.changed = c_chg != 0;
   }
   __syncthreads();
+  plap(3);
 }
 
 // FluidSim::tick (fluid.rs:564-657) for region R, n_ticks times. All threads of the CTA enter.

@@ -56,6 +56,11 @@ struct ParSmem {
   unsigned ticket;    // execution order of write groups in the segment (rollback restores the first)
 };
 
+// Per-warp cycle counters of the parallel sweep (lane 0), added to Ctl::pprof per segment.
+struct ParProf {
+  unsigned long long dep, start, load, pull, write, cells;
+};
+
 // Per-segment constants, the same on every warp.
 struct ParTick {
   unsigned seg_start, seg_end, epoch;
@@ -683,8 +688,9 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
 // running beside other warps (waits, blocking, multi-version pull reads); PM_SEQ: one warp replaying
 // a segment in order, attempts counted in `seq_pulls`. Returns false when the segment stops.
 __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* ring, const ParTick& T, int mode, unsigned i,
-                                 unsigned& seq_pulls) {
+                                 unsigned& seq_pulls, ParProf& pf) {
   const unsigned lane = lane_id();
+  long long c0 = clock64();
   const float FULL = full_level();
   const unsigned cid = key_to_id(R, R.cells[i], T.flip);
   int x, y, z;
@@ -712,6 +718,9 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
       }
     }
     if (__any_sync(FULLMASK, bad)) return false;
+    const long long c1 = clock64();
+    pf.dep += (unsigned long long)(c1 - c0);
+    c0 = c1;
     // start: pulls may hold the cell until they have written a source it reads
     bool ok = true;
     if (lane == 0) {
@@ -735,6 +744,9 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
     }
     if (!__shfl_sync(FULLMASK, ok ? 1u : 0u, 0)) return false;
     __threadfence_block();
+    const long long c2 = clock64();
+    pf.start += (unsigned long long)(c2 - c0);
+    c0 = c2;
   }
   CellRec* rc = R.rec + i;
   // ---- footprint (lane l = slot l)
@@ -750,6 +762,11 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   CD fp[7];
 #pragma unroll
   for (int l = 0; l < 7; ++l) fp[l] = shfl_cd(mine, l);
+  {
+    const long long c1 = clock64();
+    pf.load += (unsigned long long)(c1 - c0);
+    c0 = c1;
+  }
   CellOut co{0u, 0u, 0u, 0u, 0u, 0};
   bool w = false;
   float wv = 0.0f;
@@ -783,6 +800,9 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
           vol = __fadd_rn(vol, got);
           co.amask |= 2u;
         }
+        const long long c1 = clock64();
+        pf.pull += (unsigned long long)(c1 - c0);
+        c0 = c1;
       }
     }
     if (vol > 0.0f) {  // fluid.rs:602-604
@@ -857,6 +877,8 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
     else ps.state[i >> 2] = (ps.state[i >> 2] & ~(0xFFu << sh)) | (CS_DONE << sh);
   }
   __syncwarp();
+  pf.write += (unsigned long long)(clock64() - c0);
+  pf.cells += 1;
   return true;
 }
 
