@@ -709,12 +709,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         ps.viol = 0u;
         ps.viol_pos = 0xFFFFFFFFu;
         ps.ticket = 0u;
-        {
-          const unsigned e = s_end;
-          const unsigned used = R.pcnt[e] - R.pcnt[pos] + (s_mode == PM_PULL ? s_extra : 0u);
-          const unsigned room = s_c < MAX_PULLS_PER_TICK ? MAX_PULLS_PER_TICK - s_c : 0u;
-          ps.slack = (int)room - (int)used;
-        }
+        for (int w = 0; w < MAX_WARPS; ++w) ps.wrow[w] = WROW_IDLE;
         R.ctl->par_segments += 1ull;
       }
     }
@@ -748,9 +743,18 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         t = __shfl_sync(FULLMASK, t, 0);
         if (t > ps.task_end) break;
         const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
+        // publish the row and its next cell for cone_wait (key / PX = y * PZ + sorted z)
+        const unsigned ka = R.cells[a];
+        const unsigned yz = ka / (unsigned)R.PX, yy = yz / (unsigned)R.PZ, zs = yz - yy * (unsigned)R.PZ;
+        const unsigned zr = flip ? (unsigned)R.PZ - 1u - zs : zs;
+        const unsigned long long rowtag = ((unsigned long long)yy << 48) | ((unsigned long long)zr << 32);
         w_fetch += (unsigned long long)(clock64() - f0);
         bool ok = true;
-        for (unsigned i = a; i < b && ok; ++i) ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf);
+        for (unsigned i = a; i < b && ok; ++i) {
+          if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = rowtag | (R.cells[i] - yz * (unsigned)R.PX);
+          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf);
+        }
+        if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = WROW_IDLE;
         if (!ok || vld(&ps.abort)) break;
       }
       w_total += (unsigned long long)(clock64() - w0);
@@ -782,6 +786,41 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     unsigned long long att = 0;
     for (unsigned i = T.seg_start + tid; i < T.seg_end; i += NT_) att += (R.rec[i].flags & RF_ATTEMPT) ? 1u : 0u;
     att = cta_sum(sm, att);
+    const unsigned room = MAX_PULLS_PER_TICK - min(s_c, MAX_PULLS_PER_TICK);
+    if (mode == PM_PULL && att > room) {
+      // more cells attempted than the budget left (cells that pulls took below full beyond the
+      // counted ones): the cells up to the room-th attempt were right. Undo the segment and run it
+      // again up to that cell; the rest follows with the budget spent.
+      __shared__ unsigned s_cut;
+      if (tid == 0) s_cut = T.seg_end;
+      __syncthreads();
+      unsigned run = 0;
+      for (unsigned base = T.seg_start; base < T.seg_end; base += NT_) {
+        const unsigned i = base + tid;
+        const unsigned f = (i < T.seg_end && (R.rec[i].flags & RF_ATTEMPT)) ? 1u : 0u;
+        unsigned tot;
+        const unsigned off = cta_scan_count(sm, f, &tot);
+        if (f && run + off + 1u == room) s_cut = i + 1u;
+        run += tot;
+        __syncthreads();
+        if (run >= room) break;
+      }
+      rollback_segment(R, ps, ring, T.seg_start, T.seg_end, flip);
+      for (unsigned i = T.seg_start + tid; i < T.seg_end; i += NT_) atomicAnd(&ps.state[i >> 2], ~(0xFFu << ((i & 3u) * 8u)));
+      const unsigned r0 = R.rowof[T.seg_start] & 0x3FFFFFFFu, r1 = R.rowof[T.seg_end - 1u] & 0x3FFFFFFFu;
+      for (unsigned r = r0 + tid; r <= r1; r += NT_) {
+        const unsigned st = R.rowstart[r];
+        R.rowprog[r] = T.seg_start > st ? T.seg_start - st : 0u;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        R.ctl->par_rollbacks += 1ull;
+        R.ctl->par_conflicts[2] += 1ull;
+        s_cap = s_cut;
+      }
+      __syncthreads();
+      continue;
+    }
     if (tid == 0) {
       s_c += (unsigned)att;
       s_pos = T.seg_end;

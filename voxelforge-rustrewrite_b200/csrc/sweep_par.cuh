@@ -52,9 +52,19 @@ struct ParSmem {
   PullCtx pc[MAX_WARPS];
   unsigned next_task, task_end, abort, viol;
   unsigned viol_pos;  // smallest sorted position of a pull that met a conflict
-  int slack;          // attempts the segment's budget still allows beyond its counted cells
   unsigned ticket;    // execution order of write groups in the segment (rollback restores the first)
+  // the row each warp works on: y << 48 | (z - pz0) << 32 | sorted x of its next cell (x - px0, or
+  // mirrored on odd ticks); WROW_IDLE when the warp holds no row
+  unsigned long long wrow[MAX_WARPS];
 };
+constexpr unsigned long long WROW_IDLE = ~0ull;
+
+__device__ __forceinline__ unsigned sorted_xr(const Region& R, int x, bool flip) {
+  const unsigned xr = (unsigned)(x - R.px0);
+  return flip ? (unsigned)R.PX - 1u - xr : xr;
+}
+
+
 
 // Per-warp cycle counters of the parallel sweep (lane 0), added to Ctl::pprof per segment.
 struct ParProf {
@@ -117,6 +127,38 @@ __device__ __forceinline__ bool wait_done(const Region& R, ParSmem& ps, const Pa
     if (spins > 32) __nanosleep(32);
   }
   return true;
+}
+
+// Before a cell of a pull segment starts: wait while a row on a lower layer within `d` rows of z,
+// held by another warp, has not passed x + d (in sorted order). A pull's source lies above the
+// pulling cell, so cells above a row still in work would otherwise read sources before the pulls
+// that write them. Rows are taken in sorted order, so every lower-layer row is finished or held.
+// Returns false on abort or timeout.
+__device__ bool cone_wait(const Region& R, ParSmem& ps, const ParTick& T, unsigned me, int y, int z, unsigned xs, int d) {
+  const unsigned lane = lane_id();
+  bool ok = true;
+  if (lane < (unsigned)MAX_WARPS && lane != me) {
+    const unsigned zr = (unsigned)(z - R.pz0);
+    unsigned long long spins = 0;
+    while (true) {
+      const unsigned long long w = *(volatile unsigned long long*)&ps.wrow[lane];
+      if (w == WROW_IDLE) break;
+      const int wy = (int)(w >> 48), wz = (int)((w >> 32) & 0xFFFFu);
+      const unsigned wx = (unsigned)(w & 0xFFFFFFFFu);
+      if (wy >= y || abs(wz - (int)zr) > d || wx > xs + (unsigned)d) break;
+      if (vld(&ps.abort)) {
+        ok = false;
+        break;
+      }
+      if (++spins > T.spin_cap) {
+        par_timeout(R, ps, 44);
+        ok = false;
+        break;
+      }
+      if (spins > 32) __nanosleep(32);
+    }
+  }
+  return __all_sync(FULLMASK, ok);
 }
 
 // ---------------------------------------------------------------------------- world access
@@ -422,20 +464,13 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       if (cs_block(ps.state, jr)) blk = true;
       else kind = 1;
     }
-    if (lane == 0) {
-      // a drained source taken below 1 - 1e-4 attempts a pull when its turn comes: it must be
-      // among the cells counted as possible attempters (pulls take only from surface cells, so
-      // this is a cell that became a surface during the tick). In this segment that is a conflict;
-      // in a later one the cell is counted when that segment is sized.
-      if (jr != NOSLOT && jr > k && nvv < full_level() && !(R.rowof[jr] >> 31)) {
-        if (jr >= T.seg_end) {
-          if (!(atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u)) & (1u << (jr & 31u)))) {
-            const unsigned q = atomicAdd(&R.ctl->pxn, 1u);
-            if (q < MAX_CELLS_PER_TICK) R.pxlist[q] = jr;
-          }
-        } else if (atomicSub(&ps.slack, 1) <= 0) {
-          kind = 3;  // no budget left for one more attempt
-        }
+    if (lane == 0 && jr != NOSLOT && jr >= T.seg_end && nvv < full_level() && !(R.rowof[jr] >> 31)) {
+      // a drained source taken below 1 - 1e-4 attempts a pull when its turn comes; one in a later
+      // segment that was not counted as a possible attempter is counted when that segment is
+      // sized (in this segment the attempt count is checked when the segment ends)
+      if (!(atomicOr(R.pextra + (jr >> 5), 1u << (jr & 31u)) & (1u << (jr & 31u)))) {
+        const unsigned q = atomicAdd(&R.ctl->pxn, 1u);
+        if (q < MAX_CELLS_PER_TICK) R.pxlist[q] = jr;
       }
     }
     if (kind) {
@@ -721,6 +756,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
     const long long c1 = clock64();
     pf.dep += (unsigned long long)(c1 - c0);
     c0 = c1;
+    if (mode == PM_PULL && T.gate > 0 && !cone_wait(R, ps, T, threadIdx.x >> 5, y, z, sorted_xr(R, x, T.flip), T.gate)) return false;
     // start: pulls may hold the cell until they have written a source it reads
     bool ok = true;
     if (lane == 0) {
