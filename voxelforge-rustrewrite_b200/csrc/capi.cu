@@ -332,6 +332,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.pextra, (MAX_CELLS_PER_TICK + 31) / 32))) return rc;
   if ((rc = dalloc(h, &R.pxlist, MAX_CELLS_PER_TICK))) return rc;
   if ((rc = dalloc(h, &R.rb, ncells, false))) return rc;
+  if ((rc = dalloc(h, &R.deps, (uint64_t)MAX_CELLS_PER_TICK * 16, false))) return rc;
   CK(cudaMemsetAsync(R.rb, 0xFF, ncells * 4, h->stream));
   // the parallel sweep packs search-queue coordinates in 16 bits per axis
   if (R.PX >= 65536 || R.PZ >= 65536 || R.PY >= 65536) h->tune.engine = 0;

@@ -164,6 +164,7 @@ struct Region {
   unsigned* pextra;      // MAX_CELLS_PER_TICK bits: later cells a pull took below 1 - 1e-4 (not counted in pcnt)
   unsigned* pxlist;      // MAX_CELLS_PER_TICK: the positions whose pextra bit is set
   unsigned* rb;          // ncells: earliest writer during a segment's rollback (0xFFFFFFFF idle)
+  unsigned* deps;        // MAX_CELLS_PER_TICK * 16: earlier conflicting cells of each cell (10 used)
   Ctl* ctl;
 };
 

@@ -659,6 +659,11 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     R.pcnt[n] = s_pc;
     R.ctl->ptn = 0u;
   }
+  // earlier conflicting cells of every cell (the position map is complete now)
+  for (unsigned t = tid; t < n * 16u; t += NT_) {
+    const unsigned i = t >> 4, l = t & 15u;
+    R.deps[t] = l < 10u ? dep_rank(R, i, flip, l) : NOSLOT;
+  }
   for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
   for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
   if (tid == 0) R.ctl->pxn = 0u;
@@ -728,7 +733,8 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
       // one warp, in sorted order, the budget counted exactly
       if (warp == 0) {
         unsigned sp = s_c;
-        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf);
+        unsigned cgi = 0xFFFFFFFFu, cg = 0u;
+        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf, NOSLOT, cgi, cg);
         if (lane == 0) R.ctl->par_replayed += T.seg_end - T.seg_start;
       }
       __syncthreads();
@@ -750,9 +756,13 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
         const unsigned long long rowtag = ((unsigned long long)yy << 48) | ((unsigned long long)zr << 32);
         w_fetch += (unsigned long long)(clock64() - f0);
         bool ok = true;
+        unsigned cgi = 0xFFFFFFFFu, cg = 0u;
+        unsigned jr_next = R.deps[a * 16u + (lane & 15u)];
         for (unsigned i = a; i < b && ok; ++i) {
+          const unsigned jr = jr_next;
+          if (i + 1u < b) jr_next = R.deps[(i + 1u) * 16u + (lane & 15u)];  // used by the next cell
           if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = rowtag | (R.cells[i] - yz * (unsigned)R.PX);
-          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf);
+          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf, jr, cgi, cg);
         }
         if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = WROW_IDLE;
         if (!ok || vld(&ps.abort)) break;

@@ -197,6 +197,50 @@ __device__ __forceinline__ CD load_cell_par(const Region& R, const int* ring, in
   return c;
 }
 
+// load_cell_par with a one-entry cache of the lane's last grid word: a detailed brick's word (slot)
+// never changes during a sweep, so along a row the brick lookup is skipped for the cells that
+// stay in the brick of the previous cell. Uniform words are always re-read (a warp may
+// materialise the brick).
+__device__ __forceinline__ CD load_cell_cached(const Region& R, const int* ring, int x, int y, int z, unsigned long long cap, unsigned& cgi,
+                                               unsigned& cg) {
+  CD c;
+  c.part = 0.0f;
+  c.slot = NOSLOT;
+  c.gi = 0;
+  c.mat = 0;
+  c.out = outside(R, ring, x, y, z);
+  if (c.out) return c;
+  c.gi = grid_index(R, x >> 3, y >> 3, z >> 3);
+  unsigned g;
+  if (c.gi == cgi && cg >= 256u && cg != GRID_LOCKED) {
+    g = cg;
+  } else {
+    g = vld(R.grid + c.gi);
+    unsigned long long spins = 0;
+    while (g == GRID_LOCKED) {
+      if (++spins > cap) {
+        set_status(R, ST_TIMEOUT, 30);
+        c.out = true;
+        return c;
+      }
+      __nanosleep(32);
+      g = vld(R.grid + c.gi);
+    }
+    __threadfence_block();
+    cgi = c.gi;
+    cg = g;
+  }
+  if (g < 256u) {
+    c.mat = (unsigned char)g;
+    return c;
+  }
+  c.slot = g - 256u;
+  const size_t o = (size_t)c.slot * 512u + local_index(x, y, z);
+  c.mat = R.amat[o];
+  c.part = R.avol[o];
+  return c;
+}
+
 // Atlas slots for the bricks lanes with `need` are about to write (sparse_volume.rs:250-266).
 // The first warp to take a brick's grid word (CAS to GRID_LOCKED) allocates and fills the slot and
 // publishes it; the others read the published slot.
@@ -385,7 +429,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
   // sees this stamp (a conflict) or this read sees its write
   const unsigned id = dom_id(R, a, b, c);
   atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
-  __threadfence();
+  __threadfence_block();  // one CTA runs the region: CTA scope orders every party
   out = load_cell_par(R, ring, a, b, c, T.spin_cap);
   __threadfence_block();
   unsigned best = NOSLOT;
@@ -496,7 +540,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       }
       __nanosleep(32);
     }
-    __threadfence();
+    __threadfence_block();  // one CTA runs the region: CTA scope orders every party
   }
   if (!__shfl_sync(FULLMASK, locked ? 1u : 0u, 0)) {
     if (blk) cs_unblock(ps.state, jr);
@@ -532,7 +576,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
     co.src = sid;
   }
   __syncwarp();
-  __threadfence();
+  __threadfence_block();  // one CTA runs the region: CTA scope orders every party
   // a later pull that stamped its read of the source before this write saw the old value: a
   // conflict (the write is undone with the segment: the record holds the old value)
   bool late = false;
@@ -543,7 +587,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
       atomicAdd(&R.ctl->par_conflicts[1], 1ull);
       atomicMin(&ps.viol_pos, k);
     }
-    __threadfence();
+    __threadfence_block();  // one CTA runs the region: CTA scope orders every party
     atomicExch(R.rb + sid, 0xFFFFFFFFu);
   }
   if (blk) cs_unblock(ps.state, jr);
@@ -722,8 +766,10 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
 // One drained cell (fluid.rs:584-651) at sorted position i, warp-collective. PM_PULL / PM_NOPULL:
 // running beside other warps (waits, blocking, multi-version pull reads); PM_SEQ: one warp replaying
 // a segment in order, attempts counted in `seq_pulls`. Returns false when the segment stops.
+// jr: this lane's entry of the cell's earlier conflicting cells (ParDeps, lanes 0..9); cgi / cg:
+// the lane's grid-word cache (load_cell_cached).
 __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* ring, const ParTick& T, int mode, unsigned i,
-                                 unsigned& seq_pulls, ParProf& pf) {
+                                 unsigned& seq_pulls, ParProf& pf, unsigned jr, unsigned& cgi, unsigned& cg) {
   const unsigned lane = lane_id();
   long long c0 = clock64();
   const float FULL = full_level();
@@ -733,25 +779,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   // ---- earlier conflicting cells: earlier rows of the layer, the layer below, two below
   if (mode != PM_SEQ) {
     bool bad = false;
-    if (lane < 10u) {
-      int dx = 0, dy = 0, dz = 0;
-      if (lane < 4u) {
-        const int s = T.flip ? 1 : -1;
-        dz = lane == 3u ? 2 * s : s;
-        dx = lane == 0u ? -1 : (lane == 2u ? 1 : 0);
-      } else if (lane < 9u) {
-        const unsigned l = lane - 4u;
-        dy = -1;
-        dx = (l == 1u) - (l == 2u);
-        dz = (l == 3u) - (l == 4u);
-      } else {
-        dy = -2;
-      }
-      if (lane < 9u || mode == PM_PULL) {
-        const unsigned jr = rank_at(R, x + dx, y + dy, z + dz);
-        if (jr != NOSLOT && jr < i && jr >= T.seg_start && !wait_done(R, ps, T, jr, 38)) bad = true;
-      }
-    }
+    if ((lane < 9u || (lane == 9u && mode == PM_PULL)) && jr != NOSLOT && jr >= T.seg_start && !wait_done(R, ps, T, jr, 38)) bad = true;
     if (__any_sync(FULLMASK, bad)) return false;
     const long long c1 = clock64();
     pf.dep += (unsigned long long)(c1 - c0);
@@ -790,7 +818,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   fp_off((int)lane, ox, oy, oz);
   CD mine = CD{0.0f, NOSLOT, 0u, 0, true};
   if (lane < 7u) {
-    mine = load_cell_par(R, ring, x + ox, y + oy, z + oz, T.spin_cap);
+    mine = load_cell_cached(R, ring, x + ox, y + oy, z + oz, T.spin_cap, cgi, cg);
     rc->opart[lane] = mine.part;
     rc->omat[lane] = mine.mat;
   }
@@ -944,6 +972,33 @@ __device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, uns
     default: loc = cid - pxy; break;  // 6 (slot 2, up, is never written)
   }
   return true;
+}
+
+// The earlier drained cells the cell at sorted position i conflicts with (lanes 0..9 of a warp
+// hold one each; NOSLOT where there is none): earlier rows of its layer (x-1, x, x+1 one row back,
+// x two rows back, mirrored on odd ticks), the five cells of the layer below under its plus
+// footprint, and the cell two below (whose start test reads the cell this one falls into).
+__device__ __forceinline__ unsigned dep_rank(const Region& R, unsigned i, bool flip, unsigned l) {
+  const unsigned cid = key_to_id(R, R.cells[i], flip);
+  int x, y, z;
+  dom_xyz(R, cid, x, y, z);
+  int dx = 0, dy = 0, dz = 0;
+  if (l < 4u) {
+    const int s = flip ? 1 : -1;
+    dz = l == 3u ? 2 * s : s;
+    dx = l == 0u ? -1 : (l == 2u ? 1 : 0);
+  } else if (l < 9u) {
+    const unsigned q = l - 4u;
+    dy = -1;
+    dx = (q == 1u) - (q == 2u);
+    dz = (q == 3u) - (q == 4u);
+  } else if (l == 9u) {
+    dy = -2;
+  } else {
+    return NOSLOT;
+  }
+  const unsigned r = rank_at(R, x + dx, y + dy, z + dz);
+  return r < i ? r : NOSLOT;
 }
 
 // Undo the writes of segment [a, b), CTA-wide: every cell written in the segment gets back the
