@@ -201,8 +201,10 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
  * engine 1 (default): all 16 warps of the region's CTA walk rows of the sorted order at once, each
  * cell waiting for the earlier cells it conflicts with; pressure searches read cells as of their own
  * position; a segment whose order the schedule cannot keep is undone and replayed by one warp.
- * gate (0..31, default 4): before a pressure search, wait for the earlier cells of its layer within
- * this Chebyshev distance (fewer replays, later searches). spin_cap (> 0, default 2^24): iterations
+ * gate: bits 0-7 (0..31, default 4) before a pressure search, wait for the earlier cells of its layer
+ * within this Chebyshev distance; bits 8-15 (0..31, 0 = the same value) a cell of a segment with
+ * pulls starts only when rows in work on lower layers within that many rows have passed its x plus
+ * that distance (fewer replays, less overlap). spin_cap (> 0, default 2^24): iterations
  * of a device wait before the tick gives up with VF_ERR_TIMEOUT.
  * No reference counterpart: a device scheduling knob of this library. */
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap);
@@ -214,10 +216,11 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
  * (diagnostics). */
 int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3);
 
-/* Parallel-sweep SM cycle counters summed over ticks (12 entries): prepass, segments, rollbacks,
+/* Parallel-sweep SM cycle counters summed over ticks (15 entries): prepass, segments, rollbacks,
  * event logs; then summed over warps: dependency waits, blocked starts, footprint loads, pulls,
- * writes, cells run, row fetches, worker total. No reference counterpart (diagnostics). */
-int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out12);
+ * writes, cells run, row fetches, worker total, lower-layer (cone) waits, gate waits, pressure
+ * searches run. No reference counterpart (diagnostics). */
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out15);
 
 /* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
  * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */

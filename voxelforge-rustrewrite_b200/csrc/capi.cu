@@ -921,7 +921,9 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
 }
 
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap) {
-  if (!h || engine < 0 || engine > 1 || gate < 0 || gate > GATE_MAX || spin_cap == 0) return VF_ERR_INVALID;
+  if (!h || engine < 0 || engine > 1 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 16) ||
+      spin_cap == 0)
+    return VF_ERR_INVALID;
   if (engine == 1 && h->uploaded && (h->R.PX >= 65536 || h->R.PZ >= 65536 || h->R.PY >= 65536))
     return fail(h, VF_ERR_RANGE, "the parallel sweep needs domain sides below 65536");
   h->tune.engine = engine;
@@ -930,11 +932,11 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
   return VF_OK;
 }
 
-int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out12) {
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out15) {
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
-  if (out12) std::memcpy(out12, h->hctl->pprof, 12 * sizeof(uint64_t));
+  if (out15) std::memcpy(out15, h->hctl->pprof, 15 * sizeof(uint64_t));
   return VF_OK;
 }
 

@@ -597,7 +597,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
       tp0 = now;
     }
   };
-  ParProf pf{0, 0, 0, 0, 0, 0};
+  ParProf pf{0, 0, 0, 0, 0, 0, 0, 0, 0};
   unsigned long long w_fetch = 0, w_total = 0;
   // ---- positions, rows and the cells that may attempt a pull (fluid.rs:594)
   __shared__ unsigned s_rows, s_pc;
@@ -679,7 +679,8 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     s_split = 0;  // splits of the current position so far
   }
   __syncthreads();
-  const int gate = max(0, min(tune.gate, GATE_MAX));
+  const int gate = max(0, min(tune.gate & 0xFF, GATE_MAX));
+  const int cone = tune.gate >> 8 ? max(0, min((tune.gate >> 8) & 0xFF, GATE_MAX)) : gate;
   __shared__ unsigned s_extra;
   while (true) {
     // cells at or after the position that earlier pulls took below full (not counted in pcnt)
@@ -725,6 +726,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     T.seg_end = s_end;
     T.epoch = s_epoch;
     T.gate = gate;
+    T.cone = cone;
     T.flip = flip;
     T.spin_cap = tune.spin_cap;
     const int mode = (int)s_mode;
@@ -849,6 +851,9 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     atomicAdd(q + 9, pf.cells);
     atomicAdd(q + 10, w_fetch);
     atomicAdd(q + 11, w_total);
+    atomicAdd(q + 12, pf.cone);
+    atomicAdd(q + 13, pf.gate);
+    atomicAdd(q + 14, pf.npull);
   }
   tp0 = clock64();
   // ---- per-tick maps back to idle: positions, rows, pull-written cells

@@ -68,13 +68,14 @@ __device__ __forceinline__ unsigned sorted_xr(const Region& R, int x, bool flip)
 
 // Per-warp cycle counters of the parallel sweep (lane 0), added to Ctl::pprof per segment.
 struct ParProf {
-  unsigned long long dep, start, load, pull, write, cells;
+  unsigned long long dep, start, load, pull, write, cells, cone, gate, npull;
 };
 
 // Per-segment constants, the same on every warp.
 struct ParTick {
   unsigned seg_start, seg_end, epoch;
-  int gate;
+  int gate;  // same-layer radius waited for before a pressure search
+  int cone;  // lower-layer radius a cell waits for before it starts
   bool flip;
   unsigned long long spin_cap;
 };
@@ -784,7 +785,12 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
     const long long c1 = clock64();
     pf.dep += (unsigned long long)(c1 - c0);
     c0 = c1;
-    if (mode == PM_PULL && T.gate > 0 && !cone_wait(R, ps, T, threadIdx.x >> 5, y, z, sorted_xr(R, x, T.flip), T.gate)) return false;
+    if (mode == PM_PULL && T.cone > 0 && !cone_wait(R, ps, T, threadIdx.x >> 5, y, z, sorted_xr(R, x, T.flip), T.cone)) return false;
+    {
+      const long long c1 = clock64();
+      pf.cone += (unsigned long long)(c1 - c0);
+      c0 = c1;
+    }
     // start: pulls may hold the cell until they have written a source it reads
     bool ok = true;
     if (lane == 0) {
@@ -850,6 +856,12 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
       if (mode == PM_SEQ) seq_pulls += 1;
       if (pull_has_start(fp, x, z)) {
         if (mode == PM_PULL && T.gate > 0 && !gate_wait(R, ps, T, x, y, z)) return false;
+        {
+          const long long c1 = clock64();
+          pf.gate += (unsigned long long)(c1 - c0);
+          pf.npull += 1;
+          c0 = c1;
+        }
         bool ok = true;
         const float got = pull_par(R, ps, pc, ring, T, mode, i, x, y, z, __fsub_rn(1.0f, vol), fp, co, ok);
         if (!ok) {
