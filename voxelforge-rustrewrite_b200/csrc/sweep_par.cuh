@@ -83,6 +83,12 @@ struct ParTick {
 __device__ __forceinline__ unsigned vld(const unsigned* p) { return *(volatile const unsigned*)p; }
 __device__ __forceinline__ void vst(unsigned* p, unsigned v) { *(volatile unsigned*)p = v; }
 
+// Back-off of a polling loop after n polls: a few polls at full rate, then sleeps growing from 32 ns
+// to about 1 us, so waiting warps leave the issue slots to the warps that work.
+__device__ __forceinline__ void backoff(unsigned long long n) {
+  if (n > 4) __nanosleep(min(32u << (unsigned)min((n - 4) >> 2, 5ull), 1024u));
+}
+
 // ------------------------------------------------------------------------- cell states (shared)
 __device__ __forceinline__ unsigned cs_get(const unsigned* st, unsigned i) { return (vld(&st[i >> 2]) >> ((i & 3u) * 8u)) & 0xFFu; }
 // The owner's steps STARTED -> WRITING -> DONE: a byte add (the byte is >= 0xF0, no carry).
@@ -125,7 +131,7 @@ __device__ __forceinline__ bool wait_done(const Region& R, ParSmem& ps, const Pa
       par_timeout(R, ps, site);
       return false;
     }
-    if (spins > 32) __nanosleep(32);
+    backoff(spins);
   }
   return true;
 }
@@ -137,29 +143,27 @@ __device__ __forceinline__ bool wait_done(const Region& R, ParSmem& ps, const Pa
 // Returns false on abort or timeout.
 __device__ bool cone_wait(const Region& R, ParSmem& ps, const ParTick& T, unsigned me, int y, int z, unsigned xs, int d) {
   const unsigned lane = lane_id();
-  bool ok = true;
-  if (lane < (unsigned)MAX_WARPS && lane != me) {
-    const unsigned zr = (unsigned)(z - R.pz0);
-    unsigned long long spins = 0;
-    while (true) {
+  const unsigned zr = (unsigned)(z - R.pz0);
+  unsigned long long spins = 0;
+  while (true) {
+    bool held = false;
+    if (lane < (unsigned)MAX_WARPS && lane != me) {
       const unsigned long long w = *(volatile unsigned long long*)&ps.wrow[lane];
-      if (w == WROW_IDLE) break;
-      const int wy = (int)(w >> 48), wz = (int)((w >> 32) & 0xFFFFu);
-      const unsigned wx = (unsigned)(w & 0xFFFFFFFFu);
-      if (wy >= y || abs(wz - (int)zr) > d || wx > xs + (unsigned)d) break;
-      if (vld(&ps.abort)) {
-        ok = false;
-        break;
+      if (w != WROW_IDLE) {
+        const int wy = (int)(w >> 48), wz = (int)((w >> 32) & 0xFFFFu);
+        const unsigned wx = (unsigned)(w & 0xFFFFFFFFu);
+        held = wy < y && abs(wz - (int)zr) <= d && wx <= xs + (unsigned)d;
       }
-      if (++spins > T.spin_cap) {
-        par_timeout(R, ps, 44);
-        ok = false;
-        break;
-      }
-      if (spins > 32) __nanosleep(32);
     }
+    if (!__any_sync(FULLMASK, held)) return true;
+    if (vld(&ps.abort)) return false;
+    if (++spins > T.spin_cap) {
+      if (lane == 0) par_timeout(R, ps, 44);
+      __syncwarp();
+      return false;
+    }
+    backoff(spins);
   }
-  return __all_sync(FULLMASK, ok);
 }
 
 // ---------------------------------------------------------------------------- world access
@@ -183,7 +187,7 @@ __device__ __forceinline__ CD load_cell_par(const Region& R, const int* ring, in
       c.out = true;
       return c;
     }
-    __nanosleep(32);
+    backoff(spins);
     g = vld(R.grid + c.gi);
   }
   __threadfence_block();
@@ -224,7 +228,7 @@ __device__ __forceinline__ CD load_cell_cached(const Region& R, const int* ring,
         c.out = true;
         return c;
       }
-      __nanosleep(32);
+      backoff(spins);
       g = vld(R.grid + c.gi);
     }
     __threadfence_block();
@@ -261,7 +265,7 @@ __device__ void materialize_par(const Region& R, bool need, unsigned gi, unsigne
           set_status(R, ST_TIMEOUT, 31);
           break;
         }
-        __nanosleep(32);
+        backoff(spins);
         g = vld(R.grid + gi);
         continue;
       }
@@ -539,7 +543,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
         locked = false;
         break;
       }
-      __nanosleep(32);
+      backoff(spins);
     }
     __threadfence_block();  // one CTA runs the region: CTA scope orders every party
   }
@@ -724,12 +728,12 @@ __device__ float pull_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* 
 // the sources of earlier pulls there are then final. Returns false on abort.
 __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x, int y, int z) {
   const unsigned lane = lane_id();
-  bool ok = true;
+  unsigned r = NOSLOT, needc = 0;
   if ((int)lane < T.gate) {
     const int zz = T.flip ? z + 1 + (int)lane : z - 1 - (int)lane;
     const int zr = zz - R.pz0;
     if (zr >= 0 && zr < R.PZ) {
-      const unsigned r = R.zrow[(size_t)y * (unsigned)R.PZ + (unsigned)zr];
+      r = R.zrow[(size_t)y * (unsigned)R.PZ + (unsigned)zr];
       if (r != NOSLOT) {
         int xr = T.flip ? (R.PX - 1 - (x - T.gate - R.px0)) : (x + T.gate - R.px0);
         xr = min(xr, R.PX - 1);
@@ -743,25 +747,24 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
             if (R.cells[m] <= kmax) lo = m + 1u;
             else hi = m;
           }
-          const unsigned needc = lo - a;
-          unsigned long long spins = 0;
-          while (vld(R.rowprog + r) < needc) {
-            if (vld(&ps.abort)) {
-              ok = false;
-              break;
-            }
-            if (++spins > T.spin_cap) {
-              par_timeout(R, ps, 37);
-              ok = false;
-              break;
-            }
-            if (spins > 32) __nanosleep(32);
-          }
+          needc = lo - a;
         }
       }
     }
   }
-  return __all_sync(FULLMASK, ok);
+  bool pend = r != NOSLOT && needc > 0u;
+  unsigned long long spins = 0;
+  while (true) {
+    pend = pend && vld(R.rowprog + r) < needc;
+    if (!__any_sync(FULLMASK, pend)) return true;
+    if (vld(&ps.abort)) return false;
+    if (++spins > T.spin_cap) {
+      if (lane == 0) par_timeout(R, ps, 37);
+      __syncwarp();
+      return false;
+    }
+    backoff(spins);
+  }
 }
 
 // One drained cell (fluid.rs:584-651) at sorted position i, warp-collective. PM_PULL / PM_NOPULL:
@@ -779,9 +782,19 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   dom_xyz(R, cid, x, y, z);
   // ---- earlier conflicting cells: earlier rows of the layer, the layer below, two below
   if (mode != PM_SEQ) {
-    bool bad = false;
-    if ((lane < 9u || (lane == 9u && mode == PM_PULL)) && jr != NOSLOT && jr >= T.seg_start && !wait_done(R, ps, T, jr, 38)) bad = true;
-    if (__any_sync(FULLMASK, bad)) return false;
+    bool pend = (lane < 9u || (lane == 9u && mode == PM_PULL)) && jr != NOSLOT && jr >= T.seg_start;
+    unsigned long long spins = 0;
+    while (true) {
+      pend = pend && cs_get(ps.state, jr) != CS_DONE;
+      if (!__any_sync(FULLMASK, pend)) break;
+      if (vld(&ps.abort)) return false;
+      if (++spins > T.spin_cap) {
+        if (lane == 0) par_timeout(R, ps, 38);
+        __syncwarp();
+        return false;
+      }
+      backoff(spins);
+    }
     const long long c1 = clock64();
     pf.dep += (unsigned long long)(c1 - c0);
     c0 = c1;
@@ -806,7 +819,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
             ok = false;
             break;
           }
-          if (spins > 32) __nanosleep(32);
+          backoff(spins);
         }
       } else {
         atomicAdd(&ps.state[i >> 2], CS_STARTED << ((i & 3u) * 8u));
