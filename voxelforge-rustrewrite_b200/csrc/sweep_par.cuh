@@ -413,7 +413,11 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
                           int c, CD& out) {
   out = CD{0.0f, NOSLOT, 0u, 0, true};
   if (outside(R, ring, a, b, c)) return true;
-  // writers of (a, b, c): cells whose footprint slot 0, 1, 3, 4, 5 or 6 covers it (up is read only)
+  const unsigned id = dom_id(R, a, b, c);
+  // Issued together: the cell's writers among the drained cells (footprint slots 0, 1, 3..6 cover
+  // it; up is read only), its grid word, and the stamp of this read (made before the value is
+  // read: an earlier pull writes, then checks the stamp, so either it sees this stamp - a
+  // conflict - or this read sees its write).
   unsigned jr[6];
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
@@ -422,21 +426,40 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
     fp_off(fl, ox, oy, oz);
     jr[q] = rank_at(R, a - ox, b - oy, c - oz);
   }
+  out.out = false;
+  out.gi = grid_index(R, a >> 3, b >> 3, c >> 3);
+  unsigned g = vld(R.grid + out.gi);
+  atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
   if (b == ky) {
+    // earlier writers on the pulling layer must be done (those within the gate are already)
     const bool gated = T.gate > 0 && abs(a - kx) < T.gate && abs(c - kz) < T.gate;
     if (!gated) {
 #pragma unroll
       for (int q = 0; q < 6; ++q)
         if (jr[q] != NOSLOT && jr[q] < k && jr[q] >= T.seg_start && !wait_done(R, ps, T, jr[q], 34)) return false;
+      g = vld(R.grid + out.gi);  // a writer waited for may have materialised the brick
     }
   }
-  // stamp the read before making it: an earlier pull writes, then checks the stamp, so either it
-  // sees this stamp (a conflict) or this read sees its write
-  const unsigned id = dom_id(R, a, b, c);
-  atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
+  unsigned long long spins = 0;
+  while (g == GRID_LOCKED) {
+    if (++spins > T.spin_cap) {
+      set_status(R, ST_TIMEOUT, 30);
+      return false;
+    }
+    backoff(spins);
+    g = vld(R.grid + out.gi);
+  }
   __threadfence_block();  // one CTA runs the region: CTA scope orders every party
-  out = load_cell_par(R, ring, a, b, c, T.spin_cap);
+  if (g < 256u) {
+    out.mat = (unsigned char)g;
+  } else {
+    out.slot = g - 256u;
+    const size_t o = (size_t)out.slot * 512u + local_index(a, b, c);
+    out.mat = R.amat[o];
+    out.part = R.avol[o];
+  }
   __threadfence_block();
+  const unsigned ptw = vld(&R.ptbits[id >> 5]);
   unsigned best = NOSLOT;
   float bp = 0.0f;
   unsigned bm = 0;
@@ -454,7 +477,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
       bm = rc.omat[fl];
     }
   }
-  if ((vld(&R.ptbits[id >> 5]) >> (id & 31u)) & 1u) {
+  if ((ptw >> (id & 31u)) & 1u) {
     float op = 0.0f;
     unsigned om = 0;
     const unsigned w = ptreg_after(R, ps, T, id, k, op, om);
