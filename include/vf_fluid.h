@@ -216,11 +216,12 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
  * (diagnostics). */
 int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3);
 
-/* Parallel-sweep SM cycle counters summed over ticks (15 entries): prepass, segments, rollbacks,
+/* Parallel-sweep SM cycle counters summed over ticks (18 entries): prepass, segments, rollbacks,
  * event logs; then summed over warps: dependency waits, blocked starts, footprint loads, pulls,
  * writes, cells run, row fetches, worker total, lower-layer (cone) waits, gate waits, pressure
- * searches run. No reference counterpart (diagnostics). */
-int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out15);
+ * searches run, search rounds, cycles in search reads, cycles in source writes. No reference
+ * counterpart (diagnostics). */
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out18);
 
 /* Non-blocking host edits whose cell lists already live in device memory (x,y,z int32 triples),
  * for scripted runs captured in CUDA graphs: rain emitters, brush edits, wake boxes. */

@@ -388,11 +388,12 @@ class FluidSim:
         self._check(lib().vf_fluid_set_sweep(self.h, engine, gate, spin_cap), "set_sweep")
 
     SWEEP_PROFILE = ("prepass", "segments", "rollbacks", "logs", "dep_wait", "start_wait", "footprint", "pulls", "writes", "cells",
-                     "row_fetch", "worker_total", "cone_wait", "gate_wait", "searches")
+                     "row_fetch", "worker_total", "cone_wait", "gate_wait", "searches", "rounds", "search_reads",
+                     "source_writes")
 
     def sweep_profile(self) -> dict:
         """Parallel-sweep SM cycle counters summed over ticks (the per-cell ones also over warps)."""
-        a = (C.c_uint64 * 15)()
+        a = (C.c_uint64 * 18)()
         self._check(lib().vf_fluid_sweep_profile(self.h, a), "sweep_profile")
         return dict(zip(self.SWEEP_PROFILE, map(int, a)))
 

@@ -932,11 +932,11 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
   return VF_OK;
 }
 
-int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out15) {
+int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out18) {
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
-  if (out15) std::memcpy(out15, h->hctl->pprof, 15 * sizeof(uint64_t));
+  if (out18) std::memcpy(out18, h->hctl->pprof, 18 * sizeof(uint64_t));
   return VF_OK;
 }
 

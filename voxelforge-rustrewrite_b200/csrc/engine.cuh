@@ -68,7 +68,7 @@ struct Ctl {
   // parallel sweep cycle counters: 0 prepass, 1 segments (workers), 2 rollbacks, 3 event logs;
   // summed over warps: 4 dependency waits, 5 start (blocked), 6 footprint loads, 7 pulls (gate and
   // search), 8 writes, 9 cells run, 10 between cells (row fetch), 11 worker total
-  unsigned long long pprof[16];  // + 12 cone waits, 13 gate waits, 14 searches run
+  unsigned long long pprof[18];  // + 12 cone waits, 13 gate waits, 14 searches, 15 rounds, 16 reads, 17 source writes
   // SM cycles spent per tick phase, summed over ticks (clock64 on the SM running the region):
   // 0 drain, 1 sort, 2 sweep, 3 sweep waits for prefetch, 4 pressure pulls, 5 activation logs,
   // 6 writes, 7 seed commit, 8 levelling, 9 activation commit, 10 change commit, 11 mark clear

@@ -597,7 +597,7 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
       tp0 = now;
     }
   };
-  ParProf pf{0, 0, 0, 0, 0, 0, 0, 0, 0};
+  ParProf pf{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   unsigned long long w_fetch = 0, w_total = 0;
   // ---- positions, rows and the cells that may attempt a pull (fluid.rs:594)
   __shared__ unsigned s_rows, s_pc;
@@ -854,6 +854,9 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
     atomicAdd(q + 12, pf.cone);
     atomicAdd(q + 13, pf.gate);
     atomicAdd(q + 14, pf.npull);
+    atomicAdd(q + 15, pf.rounds);
+    atomicAdd(q + 16, pf.tread);
+    atomicAdd(q + 17, pf.tpw);
   }
   tp0 = clock64();
   // ---- per-tick maps back to idle: positions, rows, pull-written cells

@@ -68,7 +68,7 @@ __device__ __forceinline__ unsigned sorted_xr(const Region& R, int x, bool flip)
 
 // Per-warp cycle counters of the parallel sweep (lane 0), added to Ctl::pprof per segment.
 struct ParProf {
-  unsigned long long dep, start, load, pull, write, cells, cone, gate, npull;
+  unsigned long long dep, start, load, pull, write, cells, cone, gate, npull, rounds, tread, tpw;
 };
 
 // Per-segment constants, the same on every warp.
@@ -635,7 +635,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
 // occurrence). Entries past the 512th are never examined, so appends stop once 512 are queued.
 // Returns the volume taken; *ok = false on a conflict or abort.
 __device__ float pull_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* ring, const ParTick& T, int mode, unsigned k, int x, int y,
-                          int z, float need, const CD* fp, CellOut& co, bool& ok) {
+                          int z, float need, const CD* fp, CellOut& co, bool& ok, ParProf& pf) {
   const unsigned lane = lane_id();
   const float FULL = full_level();
   ok = true;
@@ -689,11 +689,15 @@ __device__ float pull_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* 
     }
     CD cd = CD{0.0f, NOSLOT, 0u, 0, true};
     bool rok = true;
+    const long long r0 = clock64();
     if (rd) {
       if (mode == PM_SEQ) cd = load_cell_par(R, ring, na, nb, nc, T.spin_cap);
       else rok = read_mvcc(R, ps, ring, T, k, x, y, z, na, nb, nc, cd);
     }
-    if (!__all_sync(FULLMASK, rok)) {
+    const bool allok = __all_sync(FULLMASK, rok);
+    pf.tread += (unsigned long long)(clock64() - r0);
+    pf.rounds += 1;
+    if (!allok) {
       ok = false;
       break;
     }
@@ -706,7 +710,10 @@ __device__ float pull_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* 
       const float wh = __shfl_sync(FULLMASK, here, wl);
       i += (unsigned)wl / 5u + 1u;
       const float take = fminf(need, wh);
-      if (!pull_write(R, ps, ring, T, mode, k, wa, wb, wc, __fsub_rn(wh, take), co)) {
+      const long long w0 = clock64();
+      const bool wok = pull_write(R, ps, ring, T, mode, k, wa, wb, wc, __fsub_rn(wh, take), co);
+      pf.tpw += (unsigned long long)(clock64() - w0);
+      if (!wok) {
         ok = false;
         break;
       }
@@ -899,7 +906,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
           c0 = c1;
         }
         bool ok = true;
-        const float got = pull_par(R, ps, pc, ring, T, mode, i, x, y, z, __fsub_rn(1.0f, vol), fp, co, ok);
+        const float got = pull_par(R, ps, pc, ring, T, mode, i, x, y, z, __fsub_rn(1.0f, vol), fp, co, ok, pf);
         if (!ok) {
           if (lane == 0 && !vld(&ps.abort)) {
             vst(&ps.viol, 1u);
