@@ -998,37 +998,34 @@ __device__ __forceinline__ void side4(int d, int& dx, int& dz) {  // SIDES (flui
   dz = (d == 2) - (d == 3);
 }
 
-// FluidSim::level_layer (fluid.rs:412-486), warp-cooperative. Cells are gathered in the exact
-// BFS order of the reference and summed in that order in f64.
-__device__ bool level_layer(const Region& R, WS& W, Smem& S, int sx, int sy, int sz) {
+// FluidSim::level_layer's membership test (fluid.rs:413-415) of (x, y, z): !solid && vol > 0 &&
+// supported && vol(above) <= 0. Returns the cell's volume through *v.
+__device__ __forceinline__ bool level_member(const Region& R, const int* ring, int x, int y, int z, float* v) {
+  const float FULL = full_level();
+  const CD c = load_cell(R, ring, x, y, z);
+  *v = cd_volume(c);
+  if (cd_solid(c) || !(*v > 0.0f)) return false;
+  const CD b = load_cell(R, ring, x, y - 1, z);
+  if (!(cd_solid(b) || cd_volume(b) >= FULL)) return false;
+  const CD a = load_cell(R, ring, x, y + 1, z);
+  return cd_volume(a) <= 0.0f;
+}
+
+// The flood fill of FluidSim::level_layer (fluid.rs:425-446) continued by one warp from queue
+// entry i of len (R.lvl_id / R.lvl_vol): entries are examined in order, each testing its four
+// sides once (LayerMarks) and appending the members. Stops early, with i < len, when `hand` or
+// more entries wait (the CTA takes the layer over from there). Returns the length.
+__device__ unsigned level_bfs_warp(const Region& R, Smem& S, unsigned& i, unsigned len, unsigned hand) {
   const unsigned lane = lane_id();
   const float FULL = full_level();
-  // member (fluid.rs:413-415): !solid && vol > 0 && supported && vol(above) <= 0
-  unsigned was = 0;
-  if (lane == 0) was = mark_tas(R, sx, sy, sz);
-  was = __shfl_sync(FULLMASK, was, 0);
-  if (was) return false;
-  CD m3 = CD{0.0f, NOSLOT, 0u, 0, true};
-  if (lane < 3) m3 = load_cell(R, S.ring, sx, sy + (lane == 1 ? -1 : (lane == 2 ? 1 : 0)), sz);
-  CD cs = shfl_cd(m3, 0), cb = shfl_cd(m3, 1), ca = shfl_cd(m3, 2);
-  bool member = !cd_solid(cs) && cd_volume(cs) > 0.0f && (cd_solid(cb) || cd_volume(cb) >= FULL) && cd_volume(ca) <= 0.0f;
-  if (!member) return false;
-  if (lane == 0) {
-    R.lvl_id[0] = dom_id(R, sx, sy, sz);
-    R.lvl_vol[0] = cd_volume(cs);
-  }
-  __syncwarp();
-  unsigned len = 1, i = 0;
-  double sum = 0.0;
-  float lo = 2.0f, hi = -1.0f;
   while (i < len) {
+    if (len >= MAX_LEVEL_CELLS) {  // the rest is only summed (fluid.rs:436-438)
+      i = len;
+      break;
+    }
+    if (len - i >= hand) break;
     unsigned cid = R.lvl_id[i];
-    float vol = R.lvl_vol[i];
     ++i;
-    sum = __dadd_rn(sum, (double)vol);
-    lo = fminf(lo, vol);
-    hi = fmaxf(hi, vol);
-    if (len >= MAX_LEVEL_CELLS) continue;
     int x, y, z;
     dom_xyz(R, cid, x, y, z);
     // lanes 0..11: side d = lane/3, j = lane%3 (0 the neighbour, 1 below it, 2 above it)
@@ -1056,6 +1053,65 @@ __device__ bool level_layer(const Region& R, WS& W, Smem& S, int sx, int sy, int
     len += (unsigned)__popc(pm);
     __syncwarp();
   }
+  return len;
+}
+
+// The sum and range of the gathered volumes in queue order (fluid.rs:431-434), one lane adding in
+// f64 in order; the result is broadcast to the warp.
+__device__ void level_sum_warp(const Region& R, unsigned len, double& sum, float& lo, float& hi) {
+  double s = 0.0;
+  float l = 2.0f, h = -1.0f;
+  if (lane_id() == 0) {
+    for (unsigned i = 0; i < len; ++i) {
+      const float v = R.lvl_vol[i];
+      s = __dadd_rn(s, (double)v);
+      l = fminf(l, v);
+      h = fmaxf(h, v);
+    }
+  }
+  sum = __shfl_sync(FULLMASK, s, 0);
+  lo = __shfl_sync(FULLMASK, l, 0);
+  hi = __shfl_sync(FULLMASK, h, 0);
+}
+
+// What FluidSim::level_layer does with a gathered layer (fluid.rs:446-485), one warp: count the
+// cells, then level to the average or drain the film. Returns "a voxel changed".
+__device__ bool level_finish(const Region& R, WS& W, Smem& S, unsigned len, double sum, float lo, float hi);
+
+// FluidSim::level_layer (fluid.rs:412-486), one warp. Cells are gathered in the exact BFS order of
+// the reference and summed in that order in f64. A layer whose flood fill grows to `hand` waiting
+// entries is handed over: returns true with the queue state in qi / qlen, nothing levelled yet.
+__device__ bool level_layer(const Region& R, WS& W, Smem& S, int sx, int sy, int sz, unsigned hand, unsigned& qi,
+                            unsigned& qlen) {
+  const unsigned lane = lane_id();
+  unsigned was = 0;
+  if (lane == 0) was = mark_tas(R, sx, sy, sz);
+  was = __shfl_sync(FULLMASK, was, 0);
+  if (was) return false;
+  float v0 = 0.0f;
+  const bool member = level_member(R, S.ring, sx, sy, sz, &v0);
+  if (!member) return false;
+  if (lane == 0) {
+    R.lvl_id[0] = dom_id(R, sx, sy, sz);
+    R.lvl_vol[0] = v0;
+  }
+  __syncwarp();
+  unsigned i = 0;
+  const unsigned len = level_bfs_warp(R, S, i, 1u, hand);
+  if (i < len) {
+    qi = i;
+    qlen = len;
+    return true;
+  }
+  double sum;
+  float lo, hi;
+  level_sum_warp(R, len, sum, lo, hi);
+  W.changed |= level_finish(R, W, S, len, sum, lo, hi);
+  return false;
+}
+
+__device__ bool level_finish(const Region& R, WS& W, Smem& S, unsigned len, double sum, float lo, float hi) {
+  const unsigned lane = lane_id();
   W.llc += len;
   W.level_cells_total += len;
   bool changed = false;
@@ -1137,10 +1193,12 @@ __device__ bool level_layer(const Region& R, WS& W, Smem& S, int sx, int sy, int
   return changed;
 }
 
-// FluidSim::level_surfaces (fluid.rs:489-507). Returns true when the round ended (marks to clear).
-__device__ bool level_surfaces(const Region& R, WS& W, Smem& S) {
+// FluidSim::level_surfaces (fluid.rs:489-507) on one warp, from W.llc on: pops seeds and levels
+// their layers until the budget is spent or the seeds run out (returns false; W.level_round
+// updated), or until a layer is handed over (returns true; qi / qlen as level_layer's). The caller
+// resets W.llc at the round piece's start and clears the marks when W.level_round ends false.
+__device__ __noinline__ bool level_surfaces(const Region& R, WS& W, Smem& S, unsigned hand, unsigned& qi, unsigned& qlen) {
   const unsigned lane = lane_id();
-  W.llc = 0;
   while (W.llc < LEVEL_BUDGET) {
     if (W.nseeds == 0) break;
     W.nseeds -= 1;
@@ -1162,10 +1220,10 @@ __device__ bool level_surfaces(const Region& R, WS& W, Smem& S) {
       y += steps;
       if (steps < 32) break;
     }
-    W.changed |= level_layer(R, W, S, x, y, z);
+    if (level_layer(R, W, S, x, y, z, hand, qi, qlen)) return true;
   }
   W.level_round = W.nseeds != 0;
-  return !W.level_round;
+  return false;
 }
 
 }  // namespace vfe

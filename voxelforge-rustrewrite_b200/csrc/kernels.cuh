@@ -986,6 +986,235 @@ __device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int*
   plap(3);
 }
 
+// ------------------------------------------------------------------ levelling, all warps
+// LayerMarks probe without setting (mark_tas's tile and bit); cells outside the domain read as
+// marked, as mark_tas treats them. Marks are set by atomics (in L2): read past L1.
+__device__ __forceinline__ bool mark_test(const Region& R, int x, int y, int z) {
+  if (!in_dom(R, x, y, z)) return true;
+  const unsigned xr = (unsigned)(x - R.px0), zr = (unsigned)(z - R.pz0);
+  const unsigned tile = ((zr >> 6) * (unsigned)R.PY + (unsigned)y) * (unsigned)R.TX + (xr >> 6);
+  const unsigned bit = ((zr & 63u) << 6) | (xr & 63u);
+  return (__ldcg(R.marks + (size_t)tile * 128u + (bit >> 5)) >> (bit & 31u)) & 1u;
+}
+
+// Exclusive prefix of a per-thread 64-bit value over the CTA (thread order); *total = the sum.
+__device__ unsigned long long cta_scan_u64(unsigned long long v, unsigned long long* total) {
+  __shared__ unsigned long long s_w[MAX_WARPS];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned long long incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long u = __shfl_up_sync(FULLMASK, incl, o);
+    if (lane >= (unsigned)o) incl += u;
+  }
+  if (lane == 31u) s_w[warp] = incl;
+  __syncthreads();
+  unsigned long long before = 0, all = 0;
+  for (unsigned w = 0; w < NW_; ++w) {
+    const unsigned long long t = s_w[w];
+    if (w < warp) before += t;
+    all += t;
+  }
+  __syncthreads();
+  *total = all;
+  return before + incl - v;
+}
+
+// The flood fill of FluidSim::level_layer (fluid.rs:425-446) continued from queue entry qs of qe,
+// batch by batch over the CTA. The batch is every waiting entry; entry p's side d is tried in the
+// reference's order p-major, d-minor: its rank 4(p - qs) + d claims the cell (the lowest rank is
+// the reference's first test, which sets the mark; the others find it set), and the members are
+// appended in rank order, so the queue is the reference's queue. A batch that could carry the
+// queue to MAX_LEVEL_CELLS (where the reference stops expanding part-way) finishes on one warp.
+// Returns the final length.
+__device__ __noinline__ unsigned level_bfs_cta(const Region& R, TickSmem& sm, Smem& S, unsigned qs, unsigned qe) {
+  __shared__ unsigned s_run, s_len;
+  const unsigned tid = threadIdx.x;
+  while (qs < qe) {
+    const unsigned F = qe - qs;
+    if ((unsigned long long)qe + 4ull * F >= MAX_LEVEL_CELLS) {
+      if (tid < 32u) {
+        unsigned i = qs;
+        const unsigned len = level_bfs_warp(R, S, i, qe, 0xFFFFFFFFu);
+        if (tid == 0) s_len = len;
+      }
+      __syncthreads();
+      return s_len;
+    }
+    // claims
+    for (unsigned t = tid; t < 4u * F; t += NT_) {
+      int x, y, z, dx, dz;
+      dom_xyz(R, R.lvl_id[qs + t / 4u], x, y, z);
+      side4((int)(t & 3u), dx, dz);
+      const int nx = x + dx, nz = z + dz;
+      if (R.ring_w == 0 && (nx < 0 || nz < 0)) continue;
+      if (!in_dom(R, nx, y, nz)) {  // cannot happen for neighbours of addressable cells
+        set_status(R, ST_RANGE, 8);
+        continue;
+      }
+      if (mark_test(R, nx, y, nz)) continue;
+      atomicMin(R.rb + dom_id(R, nx, y, nz), t);
+    }
+    if (tid == 0) s_run = 0;
+    __syncthreads();
+    // the winners set the mark, test and append, in rank order
+    for (unsigned base = 0; base < 4u * F; base += NT_) {
+      const unsigned t = base + tid;
+      unsigned f = 0, nid = 0;
+      float v = 0.0f;
+      if (t < 4u * F) {
+        int x, y, z, dx, dz;
+        dom_xyz(R, R.lvl_id[qs + t / 4u], x, y, z);
+        side4((int)(t & 3u), dx, dz);
+        const int nx = x + dx, nz = z + dz;
+        if (!(R.ring_w == 0 && (nx < 0 || nz < 0)) && in_dom(R, nx, y, nz)) {
+          nid = dom_id(R, nx, y, nz);
+          if (__ldcg(R.rb + nid) == t) {  // set by atomics (in L2): read past L1
+            R.rb[nid] = 0xFFFFFFFFu;
+            mark_tas(R, nx, y, nz);
+            f = level_member(R, S.ring, nx, y, nz, &v) ? 1u : 0u;
+          }
+        }
+      }
+      unsigned tot;
+      const unsigned off = cta_scan_count(sm, f, &tot);
+      if (f) {
+        R.lvl_id[qe + s_run + off] = nid;
+        R.lvl_vol[qe + s_run + off] = v;
+      }
+      __syncthreads();
+      if (tid == 0) s_run += tot;
+      __syncthreads();
+    }
+    qs = qe;
+    qe += s_run;
+    __syncthreads();
+  }
+  return qe;
+}
+
+// A layer whose one-warp flood fill has this many entries waiting continues over the CTA.
+constexpr unsigned LEVEL_HAND = 16;
+
+// Minimum and maximum of a float over the CTA.
+__device__ void cta_minmax(float& lo, float& hi) {
+  __shared__ float s_lo[MAX_WARPS], s_hi[MAX_WARPS];
+  for (int o = 16; o; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(FULLMASK, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(FULLMASK, hi, o));
+  }
+  if ((threadIdx.x & 31u) == 0) {
+    s_lo[threadIdx.x >> 5] = lo;
+    s_hi[threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  for (unsigned w = 0; w < NW_; ++w) {
+    lo = fminf(lo, s_lo[w]);
+    hi = fmaxf(hi, s_hi[w]);
+  }
+  __syncthreads();
+}
+
+// What FluidSim::level_layer does with a gathered layer of len cells (fluid.rs:430-485), over the
+// CTA. The f64 sum in queue order is formed exactly whenever every partial sum is representable:
+// all volumes are multiples of 2^L (L from the smallest, lo) and every partial sum is below
+// len * hi < 2^H, so H - L <= 53 makes each f64 addition exact and the integer sum of v / 2^L is
+// the reference's sum, in any order. Otherwise one thread adds in queue order. Levelling to the
+// average writes each cell once, in parallel, the change log in cell order; the drain branch
+// (`left` runs through the cells in order) and layers left as they are go to warp 0's
+// level_finish.
+__device__ __noinline__ void level_finish_cta(const Region& R, TickSmem& sm, WS& sW, Smem& S, unsigned len, unsigned long long cap) {
+  __shared__ double s_sum;
+  const unsigned tid = threadIdx.x;
+  float lo = 2.0f, hi = -1.0f;
+  for (unsigned k = tid; k < len; k += NT_) {
+    const float v = R.lvl_vol[k];
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+  cta_minmax(lo, hi);
+  int el, eh;
+  frexpf(lo, &el);
+  frexp((double)len * (double)hi, &eh);
+  const int L = el - 24;  // lo = m 2^el, m in [0.5, 1): its last mantissa bit is 2^(el - 24)
+  double sum;
+  if (lo >= 1.17549435e-38f && eh - L <= 53) {
+    unsigned long long q = 0;
+    for (unsigned k = tid; k < len; k += NT_) q += (unsigned long long)ldexp((double)R.lvl_vol[k], -L);
+    sum = ldexp((double)cta_sum(sm, q), L);
+  } else {
+    if (tid == 0) {
+      double a = 0.0;
+      for (unsigned k = 0; k < len; ++k) a = __dadd_rn(a, (double)R.lvl_vol[k]);
+      s_sum = a;
+    }
+    __syncthreads();
+    sum = s_sum;
+    __syncthreads();
+  }
+  const bool spread = len >= 2 && __fsub_rn(hi, lo) >= SLEEP;
+  const float avg = spread ? __double2float_rn(__ddiv_rn(sum, (double)len)) : 0.0f;
+  if (!spread || avg < MIN_SPREAD) {
+    if (tid < 32u) {
+      WS W = sW;
+      W.pdelta = 0;
+      const bool ch = level_finish(R, W, S, len, sum, lo, hi);
+      long long pd = W.pdelta;
+      for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
+      if (tid == 0) {
+        W.pdelta = sW.pdelta + pd;
+        W.changed |= ch;
+        sW = W;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    return;
+  }
+  long long pd = 0;
+  for (unsigned base = 0; base < len; base += NT_) {
+    const unsigned k = base + tid;
+    bool wv = false;
+    int x = 0, y = 0, z = 0;
+    unsigned id = 0;
+    CD c = CD{0.0f, NOSLOT, 0u, 0, true};
+    if (k < len) {
+      id = R.lvl_id[k];
+      dom_xyz(R, id, x, y, z);
+      c = load_cell_par(R, S.ring, x, y, z, cap);
+      wv = fabsf(__fsub_rn(cd_volume(c), avg)) > 1e-6f;
+    }
+    const bool need = wv && set_volume_needs_slot(c, avg);
+    if (__any_sync(FULLMASK, need)) materialize_par(R, need, c.gi, c.slot, cap);
+    bool ch = false;
+    if (wv) {
+      const SVPlan p = sv_plan(c, avg);
+      if (c.slot != NOSLOT) sv_apply(R, c, x, y, z, p);
+      ch = p.ch;
+      pd += p.dp;
+    }
+    unsigned tot;
+    const unsigned off = cta_scan(sm, ch, &tot);
+    if (ch) {
+      const unsigned pos = sW.nchg + off;
+      if (pos < R.ev_chg_cap) R.ev_chg[pos] = id;
+      else set_status(R, ST_OOM, 9);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      sW.nchg += tot;
+      if (tot) sW.changed = true;
+    }
+    __syncthreads();
+  }
+  const long long dp = (long long)cta_sum(sm, (unsigned long long)pd);
+  if (tid == 0) {
+    sW.pdelta += dp;
+    sW.llc += len;
+    sW.level_cells_total += len;
+  }
+  __syncthreads();
+}
+
 // FluidSim::tick (fluid.rs:564-657) for region R, n_ticks times. All threads of the CTA enter.
 // Per tick: drain the FIFO head and sort it (CTA), the sweep (warp 0, prefetched by the other
 // warps), the seed log's commit, levelling (warp 0), then the activation and change logs'
@@ -1008,7 +1237,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
       sm.u.s.help.qlen = sm.u.s.help.done = 0u;
     }
   }
-  __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds;
+  __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds, s_lv, s_qi, s_ql;
   __shared__ unsigned long long s_qtail;
   __shared__ WS sW;
   if (tid == 0) {
@@ -1086,21 +1315,36 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     if (tid == 0) sW.nseeds = nseeds;
     __syncthreads();
     lap(7);
-    // ---- levelling (fluid.rs:652-655), warp 0
-    if (warp == 0) {
-      WS W = sW;
+    // ---- levelling (fluid.rs:652-655): warp 0 walks the seeds; layers that grow go to the CTA
+    if (tid == 0) s_lv = (sW.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) ? 1u : 0u;
+    __syncthreads();
+    if (s_lv) {
       Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, nullptr};
-      W.pdelta = 0;
-      unsigned clear = 0;
-      if (W.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) clear = level_surfaces(R, W, S) ? 1u : 0u;
-      long long pd = W.pdelta;
-      for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
-      if (lane_id() == 0) {
-        W.pdelta = sW.pdelta + pd;
-        sW = W;
-        s_clear = clear;
+      if (tid == 0) sW.llc = 0;
+      __syncthreads();
+      while (true) {
+        if (warp == 0) {
+          WS W = sW;
+          W.pdelta = 0;
+          unsigned qi = 0, ql = 0;
+          const bool pend = level_surfaces(R, W, S, LEVEL_HAND, qi, ql);
+          long long pd = W.pdelta;
+          for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
+          if (lane_id() == 0) {
+            W.pdelta = sW.pdelta + pd;
+            sW = W;
+            s_lv = pend ? 1u : 0u;
+            s_qi = qi;
+            s_ql = ql;
+          }
+          __syncwarp();
+        }
+        __syncthreads();
+        if (!s_lv) break;
+        const unsigned len = level_bfs_cta(R, sm, S, s_qi, s_ql);
+        level_finish_cta(R, sm, sW, S, len, tune.spin_cap);
       }
-      __syncwarp();
+      if (tid == 0) s_clear = sW.level_round ? 0u : 1u;
     }
     __syncthreads();
     lap(8);
