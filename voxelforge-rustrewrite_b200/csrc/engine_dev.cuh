@@ -88,6 +88,7 @@ struct WS {
   unsigned nseeds;
   unsigned pulls;          // this tick's pull attempts (fluid.rs:583)
   unsigned llc;            // last_level_cells
+  unsigned ndrain;         // layers drained to a film (fluid.rs:456-481) since the handle's start
   unsigned epoch;          // press-BFS visited epoch
   bool level_round;
   bool changed;
@@ -1131,6 +1132,7 @@ __device__ bool level_finish(const Region& R, WS& W, Smem& S, unsigned len, doub
         changed |= warp_set_volume(R, W, wv, c, x, y, z, avg);
       }
     } else {  // drain into the water under the film (fluid.rs:456-481)
+      W.ndrain += 1;
       double left = sum;
       bool stop = false;
       for (unsigned b0 = 0; b0 < len && !stop; b0 += 32) {
@@ -1191,39 +1193,6 @@ __device__ bool level_finish(const Region& R, WS& W, Smem& S, unsigned len, doub
     }
   }
   return changed;
-}
-
-// FluidSim::level_surfaces (fluid.rs:489-507) on one warp, from W.llc on: pops seeds and levels
-// their layers until the budget is spent or the seeds run out (returns false; W.level_round
-// updated), or until a layer is handed over (returns true; qi / qlen as level_layer's). The caller
-// resets W.llc at the round piece's start and clears the marks when W.level_round ends false.
-__device__ __noinline__ bool level_surfaces(const Region& R, WS& W, Smem& S, unsigned hand, unsigned& qi, unsigned& qlen) {
-  const unsigned lane = lane_id();
-  while (W.llc < LEVEL_BUDGET) {
-    if (W.nseeds == 0) break;
-    W.nseeds -= 1;
-    unsigned k = R.seeds[W.nseeds];
-    if (lane == 0) atomicAnd(&R.seedbits[k >> 5], ~(1u << (k & 31)));
-    __syncwarp();
-    int x, y, z;
-    dom_xyz(R, k, x, y, z);
-    // walk up to the top water cell (fluid.rs:496-499), 32 cells per round
-    while (true) {
-      int yy = y + 1 + (int)lane;
-      bool cond = false;
-      if (yy < R.ny) {
-        CD c = load_cell(R, S.ring, x, yy, z);
-        cond = !cd_solid(c) && cd_volume(c) > 0.0f;
-      }
-      unsigned fail = __ballot_sync(FULLMASK, !cond);
-      int steps = fail ? __ffs(fail) - 1 : 32;
-      y += steps;
-      if (steps < 32) break;
-    }
-    if (level_layer(R, W, S, x, y, z, hand, qi, qlen)) return true;
-  }
-  W.level_round = W.nseeds != 0;
-  return false;
 }
 
 }  // namespace vfe

@@ -188,6 +188,7 @@ __device__ void load_ws(const Region& R, WS& W) {
   W.nseeds = c.nseeds;
   W.pulls = 0;
   W.llc = c.last_level_cells;
+  W.ndrain = 0;
   W.epoch = 1;
   W.level_round = c.level_round != 0;
   W.changed = false;
@@ -585,7 +586,7 @@ __device__ unsigned long long cta_sum(TickSmem& sm, unsigned long long v) {
 // The sweep of one tick by every warp of the CTA (sweep_par.cuh describes the schedule). On return
 // the tick's activation, seed and change logs hold the sweep's events in program order and sW its
 // counters, exactly as the one-warp sweep leaves them.
-__device__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
+__device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& sW, const int* ring, unsigned n, bool flip, Tune tune) {
   ParSmem& ps = sm.u.p;
   const unsigned tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const float FULL = full_level();
@@ -1215,6 +1216,122 @@ __device__ __noinline__ void level_finish_cta(const Region& R, TickSmem& sm, WS&
   __syncthreads();
 }
 
+// FluidSim::level_surfaces (fluid.rs:489-507) from sW.llc on, over the CTA, in batches of up to one
+// seed per thread (LIFO order = thread order). Every thread walks its seed up to the top water cell
+// (fluid.rs:496-499) and tests the start: a start that is marked, repeats an earlier start of the
+// batch, or is not a layer member needs no flood fill. Levelling a layer to its average changes no
+// cell's solidity, its "vol > 0" or "supported", so these tests stay true while the batch's
+// earlier layers are levelled; a drained layer (which can change them) ends the batch. The
+// remaining starts, the candidates, are levelled in order (warp 0, handing grown layers to the
+// CTA), each marked at its turn as the reference does; the budget (fluid.rs:492) ends the batch
+// after the candidate that spends it. The popped seeds leave the seed set and their starts are
+// marked (a start that is not a member is marked, and skipped by every later flood fill, either
+// way). sW.level_round is updated at the end.
+__device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& sW, Smem& S, unsigned long long cap) {
+  __shared__ unsigned s_ns, s_stop, s_brk, s_pend, s_qi, s_ql;
+  const unsigned tid = threadIdx.x;
+  unsigned* b_start = sm.hist;          // the batch's starts (domain ids), by seed
+  unsigned* b_cand = sm.hist + NT_;     // candidate seeds in order
+  while (true) {
+    if (tid == 0) s_ns = (sW.llc < LEVEL_BUDGET) ? sW.nseeds : 0u;
+    __syncthreads();
+    const unsigned ns = s_ns;
+    if (ns == 0u) break;
+    const unsigned B = min(ns, NT_);
+    // ---- starts and their tests, one seed per thread
+    unsigned sid = 0;
+    int x = 0, y = 0, z = 0;
+    if (tid < B) {
+      dom_xyz(R, R.seeds[ns - 1u - tid], x, y, z);
+      while (true) {  // four cells of the column per step
+        bool up[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int yy = y + 1 + q;
+          up[q] = false;
+          if (yy < R.ny) {
+            const CD c = load_cell(R, S.ring, x, yy, z);
+            up[q] = !cd_solid(c) && cd_volume(c) > 0.0f;
+          }
+        }
+        const int steps = !up[0] ? 0 : !up[1] ? 1 : !up[2] ? 2 : !up[3] ? 3 : 4;
+        y += steps;
+        if (steps < 4) break;
+      }
+      sid = dom_id(R, x, y, z);
+      b_start[tid] = sid;
+      atomicMin(R.rb + sid, tid);
+    }
+    __syncthreads();
+    const bool first = tid < B && __ldcg(R.rb + sid) == tid;  // set by atomics (in L2): read past L1
+    __syncthreads();
+    unsigned cand = 0;
+    if (first) {
+      R.rb[sid] = 0xFFFFFFFFu;
+      float v;
+      cand = (!mark_test(R, x, y, z) && level_member(R, S.ring, x, y, z, &v)) ? 1u : 0u;
+    }
+    unsigned nc;
+    const unsigned off = cta_scan_count(sm, cand, &nc);
+    if (cand) b_cand[off] = tid;
+    if (tid == 0) {
+      s_stop = B;
+      s_brk = 0;
+    }
+    __syncthreads();
+    // ---- the candidates in order
+    for (unsigned c = 0; c < nc; ++c) {
+      const unsigned j = b_cand[c];
+      if (tid < 32u) {
+        WS W = sW;
+        W.pdelta = 0;
+        int cx, cy, cz;
+        dom_xyz(R, b_start[j], cx, cy, cz);
+        unsigned qi = 0, ql = 0;
+        const bool pend = level_layer(R, W, S, cx, cy, cz, LEVEL_HAND, qi, ql);
+        long long pd = W.pdelta;
+        for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
+        if (tid == 0) {
+          W.pdelta = sW.pdelta + pd;
+          sW = W;
+          s_pend = pend ? 1u : 0u;
+          s_qi = qi;
+          s_ql = ql;
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      if (s_pend) {
+        const unsigned len = level_bfs_cta(R, sm, S, s_qi, s_ql);
+        level_finish_cta(R, sm, sW, S, len, cap);
+      }
+      if (tid == 0 && (sW.llc >= LEVEL_BUDGET || sW.ndrain != 0u)) {
+        s_stop = j + 1u;
+        s_brk = 1u;
+      }
+      __syncthreads();
+      if (s_brk) break;
+    }
+    // ---- the popped seeds
+    const unsigned stop = s_stop;
+    if (tid < stop) {
+      const unsigned k = R.seeds[ns - 1u - tid];
+      atomicAnd(&R.seedbits[k >> 5], ~(1u << (k & 31u)));
+      int sx, sy, sz;
+      dom_xyz(R, b_start[tid], sx, sy, sz);
+      mark_tas(R, sx, sy, sz);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      sW.nseeds = ns - stop;
+      sW.ndrain = 0u;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) sW.level_round = sW.nseeds != 0u;
+  __syncthreads();
+}
+
 // FluidSim::tick (fluid.rs:564-657) for region R, n_ticks times. All threads of the CTA enter.
 // Per tick: drain the FIFO head and sort it (CTA), the sweep (warp 0, prefetched by the other
 // warps), the seed log's commit, levelling (warp 0), then the activation and change logs'
@@ -1237,7 +1354,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
       sm.u.s.help.qlen = sm.u.s.help.done = 0u;
     }
   }
-  __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds, s_lv, s_qi, s_ql;
+  __shared__ unsigned s_n, s_flip, s_clear, s_abort, s_nseeds, s_lv;
   __shared__ unsigned long long s_qtail;
   __shared__ WS sW;
   if (tid == 0) {
@@ -1315,35 +1432,14 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     if (tid == 0) sW.nseeds = nseeds;
     __syncthreads();
     lap(7);
-    // ---- levelling (fluid.rs:652-655): warp 0 walks the seeds; layers that grow go to the CTA
+    // ---- levelling (fluid.rs:652-655)
     if (tid == 0) s_lv = (sW.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) ? 1u : 0u;
     __syncthreads();
     if (s_lv) {
       Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, nullptr};
       if (tid == 0) sW.llc = 0;
       __syncthreads();
-      while (true) {
-        if (warp == 0) {
-          WS W = sW;
-          W.pdelta = 0;
-          unsigned qi = 0, ql = 0;
-          const bool pend = level_surfaces(R, W, S, LEVEL_HAND, qi, ql);
-          long long pd = W.pdelta;
-          for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
-          if (lane_id() == 0) {
-            W.pdelta = sW.pdelta + pd;
-            sW = W;
-            s_lv = pend ? 1u : 0u;
-            s_qi = qi;
-            s_ql = ql;
-          }
-          __syncwarp();
-        }
-        __syncthreads();
-        if (!s_lv) break;
-        const unsigned len = level_bfs_cta(R, sm, S, s_qi, s_ql);
-        level_finish_cta(R, sm, sW, S, len, tune.spin_cap);
-      }
+      level_round_cta(R, sm, sW, S, tune.spin_cap);
       if (tid == 0) s_clear = sW.level_round ? 0u : 1u;
     }
     __syncthreads();
