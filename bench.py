@@ -1,15 +1,18 @@
 """Benchmark: cell-steps/s of the CA-water tick on B200, bit-exact engine.
 
-One step = one tick of the dam-break workload (512x128x512 voxels, noise terrain, lake below
-y=48, 8-wide channel carved to y=30; the 1000-tick scenario) through the engine's C ABI. The
-unit of work is the cell-step: one cell drained and processed by the tick's main loop (the
-reference's last_tick_cells, summed), identical for CPU and GPU because results are bit-exact.
+Workload: the dam break (512x128x512 voxels, 4-octave noise terrain, lake below y=48, 8-wide
+channel carved to y=30; a 1000-tick scenario). One step = one levelling period of the scenario,
+10 ticks (FluidSim levels every 10th tick, fluid.rs:652-655), so every step holds the same mix of
+sweeps and levelling. The unit of work is the cell-step: one cell drained and processed by a
+tick's main loop (the reference's last_tick_cells, summed), identical on CPU and GPU because the
+results are bit-exact (the window's end state is checked against the CPU oracle in the run).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --suite      # every workload: CPU oracle (1 thread, all threads), plain GPU,
-                               # batched + CUDA graph, batched + learned proposal; one JSON line each
 
-Multi-GPU runs replicas (a single world does not shard): every rank steps its own copy, and
+`--impl reference` times the CPU restatement of fluid.rs (the oracle) on the same window of the
+same workload, built from the same inputs (oracle/_build/libvf_inputs.so; the engine's library is
+not loaded). The dam break is one world: its sweep is sequential by definition, so the reference
+runs on one core. Multi-GPU runs replicas (a world does not shard): every rank steps its own copy,
 value = all ranks' cell-steps / the slowest rank's device time.
 """
 from __future__ import annotations
@@ -29,23 +32,36 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "cell-steps/s on 1 B200 (bit-exact): learned+batched vs plain GPU CA vs fluid.rs CPU"
 UNIT = "cell-steps/s"
-WORKLOAD = {"workload": "dam-break 512x128x512, noise terrain, lake y<48, 8-wide channel to y=30", "ticks_scenario": 1000}
+TICKS_PER_STEP = 10
+DAM_BREAK = "dam-break 512x128x512, 4-octave noise terrain, lake y<48, 8-wide channel to y=30"
+# DRAM bytes (read + write) of one k_tick_par launch of one step (10 dam-break ticks, ticks
+# 51..60, cold L2 as after the bench's flush): a one-off ncu capture, summarised in
+# profiles/k_tick_par_dambreak_step_dram.txt. Compare with roofline.alg_bytes_per_step.
+STEP_DRAM_BYTES = 2013184 + 111360
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20, help="timed steps of 10 ticks")
+    ap.add_argument("--warmup", type=int, default=5, help="untimed steps of 10 ticks before them")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--engine", type=int, default=1, help="0: one-warp sweep, 1: parallel sweep")
+    ap.add_argument("--gate", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--suite", action="store_true")
-    ap.add_argument("--suite-only", default="", help="comma-separated workload ids for --suite")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--variant-ticks", type=int, default=100)
     return ap.parse_args()
+
+
+def config(args) -> dict:
+    """The workload and window both arms time (identical dicts)."""
+    name = DAM_BREAK if (args.workload, args.scale) == (2, 1.0) else f"workload {args.workload} at scale {args.scale}"
+    w0 = args.warmup * TICKS_PER_STEP
+    return {"workload": name, "ticks_scenario": 1000, "ticks_per_step": TICKS_PER_STEP, "timed_ticks": [w0 + 1, w0 + args.steps * TICKS_PER_STEP],
+            "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas (one world per GPU)"}
 
 
 def peaks():
@@ -107,213 +123,161 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_oracle(args, ticks_timed, warm):
-    """The CPU restatement of fluid.rs on this host: same workload, same ticks; 1 core."""
+# ------------------------------------------------------------------------------ CPU oracle
+def _oracle_modules():
     import __graft_entry__ as ge
 
-    vf, orc = ge.load_package(), ge.load_oracle()
+    return ge.load_oracle(), ge.load_oracle_inputs()
+
+
+def oracle_window(wid: int, scale: float, warm: int, ticks: int, reps: int = 1):
+    """Region 0 of workload `wid` on the CPU oracle (1 thread): `warm` ticks, then `ticks` timed
+    ticks (the same host-edit script as the engine's runs). Returns the median of `reps` runs as
+    (cell-steps/s, cell-steps, seconds, end-state digest)."""
+    orc, oin = _oracle_modules()
+    inp = oin.Inputs(wid, scale, 1)
+    runs = []
+    for _ in range(reps):
+        o = oin.oracle_for(orc, inp, 0)
+        em = inp.emitters(0)
+        for t in range(warm):
+            oin.script_step(o, inp, 0, t, em)
+        c0 = o.stats()["cells"]
+        if not inp.emit_every and not inp.edit_every:
+            secs = o.time_ticks(ticks)
+        else:
+            t0 = time.perf_counter()
+            for t in range(warm, warm + ticks):
+                oin.script_step(o, inp, 0, t, em)
+            secs = time.perf_counter() - t0
+        cells = o.stats()["cells"] - c0
+        runs.append((cells / secs, cells, secs, o.digest()))
+        del o
+    return sorted(runs)[len(runs) // 2]
+
+
+def oracle_regions(wid: int, scale: float, ticks: int, threads: int, regions=None):
+    """Regions of workload `wid` on the CPU oracle, ticks 0..ticks, `threads` host threads (one
+    region per task; the oracle releases the GIL in its calls). Returns (cell-steps/s by wall time
+    of the pool, cell-steps, seconds, {region: digest})."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    orc, oin = _oracle_modules()
+    inp = oin.Inputs(wid, scale, 1)
+    regions = list(range(inp.regions)) if regions is None else list(regions)
+    built = {r: oin.oracle_for(orc, inp, r) for r in regions}  # built before the clock starts
+    emit = {r: inp.emitters(r) for r in regions}
+
+    def run(r):
+        o = built[r]
+        for t in range(ticks):
+            oin.script_step(o, inp, r, t, emit[r])
+        return r, o.stats()["cells"], o.digest()
+
+    t0 = time.perf_counter()
+    if threads <= 1:
+        res = [run(r) for r in regions]
+    else:
+        with ThreadPoolExecutor(threads) as ex:
+            res = list(ex.map(run, regions))
+    secs = time.perf_counter() - t0
+    cells = sum(c for _, c, _ in res)
+    return cells / secs, cells, secs, {r: d for r, _, d in res}
+
+
+# ------------------------------------------------------------------------------- variants
+VARIANTS = [
+    (3, "64 regions, x,z in 32..256, y in 64..128, noise terrain, 1-4 water boxes (one persistent launch)"),
+    (4, "ring 9x9 chunks of 128x256x128 (1152x256x1152), sea y<64, 1000 rain emitters, 1 level per 4 ticks"),
+]
+VARIANT_TUNE = [{"engine": 0, "producers": 7, "depth": 64, "ticks_per_launch": 10}, {"engine": 1, "gate": 4, "ticks_per_launch": 10},
+                {"engine": 1, "gate": 8, "ticks_per_launch": 10}]
+
+
+def _digests(sims):
+    return [s.digest() for s in sims]
+
+
+def variant_row(vf, torch, stream, wid: int, desc: str, ticks: int, mlp, threads: int) -> dict:
+    """Workload `wid` at full size over ticks 0..ticks through the three execution modes (plain,
+    batched CUDA graph with autotuned knobs, batched + learned proposal), each checked against the
+    CPU oracle's end state, next to the oracle on 1 thread and on all host threads."""
+    from vfwater import autotune, runner
+
+    wl = vf.Workload(wid, 1.0, 1)
+    row = {"workload": desc, "regions": wl.regions, "ticks": [1, ticks]}
+    knobs = None
+    if wl.regions > 1:
+        knobs, table = autotune.tune(vf, wid, 1.0, torch, warmup=0, ticks=10, candidates=VARIANT_TUNE)
+        row["tuned"] = knobs
+        row["tune_table"] = [{k: r[k] for k in ("engine", "gate", "producers", "depth", "cell_steps_per_s")} for r in table]
+    sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=knobs)
+    plain = runner.run_plain(vf, wl, sims, 0, ticks, torch, stream)
+    d_plain = _digests(sims)
+    for s in sims:
+        s.close()
+    sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=knobs)
+    bat = runner.run_batched(vf, wl, sims, 0, ticks, torch, stream)
+    d_bat = _digests(sims)
+    for s in sims:
+        s.close()
+    sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=knobs)
+    lr = runner.run_learned(vf, wl, sims, 0, ticks, torch, stream, mlp)
+    d_lr = _digests(sims)
+    for s in sims:
+        s.close()
+    row.update({"plain": plain.cell_steps_per_s, "batched_graph": bat.cell_steps_per_s, "batched_graph_learned": lr.run.cell_steps_per_s,
+                "cell_steps": bat.cells, "batched_over_plain": bat.cell_steps_per_s / plain.cell_steps_per_s,
+                "learned_over_batched": lr.run.cell_steps_per_s / bat.cell_steps_per_s,
+                "learned": {"recall": lr.recall, "precision": lr.precision, "staged_bricks": lr.staged, "scored": lr.scored,
+                            "stage_share": lr.stage_seconds / lr.run.seconds if lr.run.seconds else None}})
+    # the CPU oracle: all regions on all host threads (also the end-state check), 1 thread on a
+    # sample of up to 4 regions
+    v_all, c_all, s_all, d_orc = oracle_regions(wid, 1.0, ticks, threads)
+    same = all(d_orc[r] == d_plain[r] == d_bat[r] == d_lr[r] for r in range(wl.regions))
+    sample = list(range(min(4, wl.regions)))
+    v1, c1, s1, _ = oracle_regions(wid, 1.0, ticks, 1, regions=sample)
+    row["cpu_all_threads"] = {"value": v_all, "unit": UNIT, "cores": threads, "kind": "port", "cell_steps": c_all, "seconds": s_all,
+                              "sample": f"all {wl.regions} regions, ticks 1..{ticks}, one region per task, wall time of the pool"}
+    row["cpu_1thread"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port", "cell_steps": c1, "seconds": s1,
+                          "sample": f"regions {sample[0]}..{sample[-1]}, ticks 1..{ticks}, one after another"}
+    row["oracle_digest_match"] = bool(same)
+    return row
+
+
+def headline_variants(vf, torch, stream, args, mlp) -> dict:
+    """The headline window again through the batched CUDA-graph path and batched + learned."""
+    from vfwater import runner
+
     wl = vf.Workload(args.workload, args.scale, 1)
-    w = wl.world(0)
-    i = w.info
-    grid, bricks, ring = w.arrays()
-    o = orc.Oracle.from_arrays((i.nx, i.ny, i.nz, i.ring_w), grid, bricks, ring)
-    for b in wl.wakes(0):
-        o.wake(*map(int, b))
-    o.tick(warm)
-    c0 = o.stats()["cells"]
-    secs = o.time_ticks(ticks_timed)
-    cells = o.stats()["cells"] - c0
-    return cells / secs, cells, secs
-
-
-CPU_SAMPLE_TICKS = 500
-# DRAM bytes (read + write) of one k_tick launch of one dam-break tick, from an ncu capture
-# (profiles/k_tick_dambreak_full_capture.txt); compare with roofline.alg_bytes_per_step.
-TICK_DRAM_BYTES = 636672
-
-
-def variants(args, vf, wl, torch, stream):
-    """The headline workload's timed ticks again through the batched CUDA-graph path and the
-    batched + learned-proposal path (fresh sims, same warm-up, same ticks; device time)."""
-    from vfwater import proposal, runner
-
+    w0, nt = args.warmup * TICKS_PER_STEP, args.steps * TICKS_PER_STEP
+    knobs = {"engine": args.engine, "gate": args.gate}
     out = {}
-    sims = runner.make_sims(vf, wl, stream.cuda_stream)
-    runner.run_batched(vf, wl, sims, 0, args.warmup, torch, stream)
-    r = runner.run_batched(vf, wl, sims, args.warmup, args.steps, torch, stream)
-    out["batched_graph"] = r.cell_steps_per_s
-    for s_ in sims:
-        s_.close()
-    mlp, info = proposal.train_default(vf, torch)
-    sims = runner.make_sims(vf, wl, stream.cuda_stream)
-    runner.run_batched(vf, wl, sims, 0, args.warmup, torch, stream)
-    lr = runner.run_learned(vf, wl, sims, args.warmup, args.steps, torch, stream, mlp)
+    sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=knobs)
+    runner.run_batched(vf, wl, sims, 0, w0, torch, stream)
+    out["batched_graph"] = runner.run_batched(vf, wl, sims, w0, nt, torch, stream).cell_steps_per_s
+    for s in sims:
+        s.close()
+    sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=knobs)
+    runner.run_batched(vf, wl, sims, 0, w0, torch, stream)
+    lr = runner.run_learned(vf, wl, sims, w0, nt, torch, stream, mlp)
     out["batched_graph_learned"] = lr.run.cell_steps_per_s
     out["learned"] = {"recall": lr.recall, "precision": lr.precision, "scored": lr.scored, "staged": lr.staged,
-                      "stage_share": lr.stage_seconds / lr.run.seconds if lr.run.seconds else None,
-                      "heldout": info["heldout"], "persistence": info["persistence"]}
-    for s_ in sims:
-        s_.close()
-    mlp.close()
+                      "stage_share": lr.stage_seconds / lr.run.seconds if lr.run.seconds else None}
+    for s in sims:
+        s.close()
     return out
 
 
-# --suite: (workload id, description, warm-up ticks, timed window of ticks). Every variant runs the
-# same window from the same state, so the cell-steps are identical and the rates compare directly.
-SUITE = [
-    (1, "basin 64^3, 16^3 water block", 0, 300),
-    (2, "dam break 512x128x512", 10, 100),
-    (3, "64 regions x,z in 32..256, y in 64..128, 1-4 water boxes", 0, 10),
-    (4, "ring 9x9 chunks of 128x256x128, sea y<64, 1000 rain emitters", 0, 40),
-    (5, "64 regions + sphere carve/fill every 10 ticks", 0, 10),
-]
-
-
-SUITE_TUNE_CANDIDATES = [{"producers": p, "depth": d, "ticks_per_launch": 4} for p in (4, 7) for d in (16, 64)]
-
-
-def oracle_script(orc, wl, r, warm, ticks):
-    """Region r of the workload on the CPU oracle: warm-up, then the timed window with the same
-    emitter and edit script as the GPU runs. Returns (cell-steps, seconds, state digest)."""
-    w = wl.world(r)
-    i = w.info
-    grid, bricks, ring = w.arrays()
-    o = orc.Oracle.from_arrays((i.nx, i.ny, i.nz, i.ring_w), grid, bricks, ring)
-    for b in wl.wakes(r):
-        o.wake(*map(int, b))
-    em, amt = wl.emitters(r)
-
-    def step(t):
-        if wl.emit_every and t % wl.emit_every == 0 and len(em):
-            o.emit(em, amt)
-        if wl.edit_every and t % wl.edit_every == wl.edit_every - 1:
-            ed = wl.edit(r, t)
-            if ed is not None:
-                o.apply_brush(ed[0], ed[1])
-                o.wake(*map(int, ed[2]))
-        o.tick()
-
-    for t in range(warm):
-        step(t)
-    c0 = o.stats()["cells"]
-    if not wl.emit_every and not wl.edit_every:
-        secs = o.time_ticks(ticks)
-    else:
-        t0 = time.perf_counter()
-        for t in range(warm, warm + ticks):
-            step(t)
-        secs = time.perf_counter() - t0
-    cells = o.stats()["cells"] - c0
-    d = o.digest()
-    del o
-    return cells, secs, d
-
-
-def cpu_suite_row(orc, wl, warm, ticks, threads):
-    """All regions on the oracle with `threads` host threads (one region per task; the oracle
-    releases the GIL inside its calls). Returns (cell-steps/s, cell-steps, seconds, digests)."""
-    from concurrent.futures import ThreadPoolExecutor
-
-    t0 = time.perf_counter()
-    if threads == 1:
-        res = [oracle_script(orc, wl, r, warm, ticks) for r in range(wl.regions)]
-        secs = sum(x[1] for x in res)  # timed ticks only
-    else:
-        with ThreadPoolExecutor(threads) as ex:
-            res = list(ex.map(lambda r: oracle_script(orc, wl, r, warm, ticks), range(wl.regions)))
-        secs = time.perf_counter() - t0  # wall time of the whole pool (includes set-up)
-    cells = sum(x[0] for x in res)
-    return cells / secs, cells, secs, [x[2] for x in res]
-
-
-def suite(args):
-    """One JSON line per workload: CPU oracle 1 thread / all threads, plain GPU, batched + CUDA
-    graph, batched + learned proposal, roofline fraction, recall/precision; states cross-checked."""
-    import torch
-
-    import __graft_entry__ as ge
-
-    vf, orc = ge.load_package(), ge.load_oracle()
-    from vfwater import autotune, proposal, runner
-
-    torch.cuda.set_device(0)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    peak, peak_kind = peaks()
-    threads = os.cpu_count() or 1
-    mlp, info = proposal.train_default(vf, torch)
-    print(json.dumps({"suite": "proposal training", "samples": info["samples"], "collect_s": info["collect_s"], "train_s": info["train_s"],
-                      "loss_first": info["loss_first"], "loss_last": info["loss_last"], "heldout": info["heldout"],
-                      "persistence": info["persistence"]}), flush=True)
-    only = {int(x) for x in args.suite_only.split(",") if x}
-    for wid, desc, warm, ticks in SUITE:
-        if only and wid not in only:
-            continue
-        wl = vf.Workload(wid, 1.0, 1)
-        row = {"suite": wid, "workload": desc, "regions": wl.regions, "warmup_ticks": warm, "ticks": ticks, "unit": UNIT}
-        # batched runs use the autotuner's knobs for many-region workloads (timed on a short window)
-        tune = None
-        if wl.regions > 1:
-            best, _ = autotune.tune(vf, wid, 1.0, torch, warmup=2, ticks=4, candidates=SUITE_TUNE_CANDIDATES)
-            tune = (best["producers"], best["depth"])
-            row["tuned"] = best
-        # GPU: plain (one region per launch, one tick per launch, host waits each tick)
-        sims = runner.make_sims(vf, wl, stream.cuda_stream)
-        if warm:
-            runner.run_batched(vf, wl, sims, 0, warm, torch, stream)
-        s0 = [s.stats() for s in sims]
-        with Clocks(0) as clk:
-            plain = runner.run_plain(vf, wl, sims, warm, ticks, torch, stream)
-        s1 = [s.stats() for s in sims]
-        dig_plain = [s.digest() for s in sims]
-        lvl = sum(b.level_cells_total - a.level_cells_total for a, b in zip(s0, s1))
-        bfs = sum(b.bfs_visits - a.bfs_visits for a, b in zip(s0, s1))
-        for s_ in sims:
-            s_.close()
-        # GPU: batched, whole window as one CUDA graph
-        sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
-        if warm:
-            runner.run_batched(vf, wl, sims, 0, warm, torch, stream)
-        bat = runner.run_batched(vf, wl, sims, warm, ticks, torch, stream)
-        dig_bat = [s.digest() for s in sims]
-        for s_ in sims:
-            s_.close()
-        # GPU: batched + learned proposal
-        sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
-        if warm:
-            runner.run_batched(vf, wl, sims, 0, warm, torch, stream)
-        lr = runner.run_learned(vf, wl, sims, warm, ticks, torch, stream, mlp)
-        dig_lr = [s.digest() for s in sims]
-        for s_ in sims:
-            s_.close()
-        # CPU oracle
-        c1, cells1, secs1, dig_cpu = cpu_suite_row(orc, wl, warm, ticks, 1)
-        cn = None
-        if wl.regions > 1:
-            cn, _, _, _ = cpu_suite_row(orc, wl, warm, ticks, threads)
-        same = dig_plain == dig_bat == dig_lr == dig_cpu
-        alg = 10.0 * plain.cells + 5.0 * lvl + 5.0 * bfs
-        row.update({
-            "cell_steps": plain.cells, "bit_exact_all_variants_vs_oracle": same,
-            "cpu_1_thread": c1, "cpu_all_threads": cn, "cpu_threads": threads,
-            "plain_gpu": plain.cell_steps_per_s, "batched_graph": bat.cell_steps_per_s, "batched_learned": lr.run.cell_steps_per_s,
-            "batched_over_plain": bat.cell_steps_per_s / plain.cell_steps_per_s if plain.cell_steps_per_s else None,
-            "learned_over_plain": lr.run.cell_steps_per_s / plain.cell_steps_per_s if plain.cell_steps_per_s else None,
-            "recall": lr.recall, "precision": lr.precision, "staged_bricks": lr.staged,
-            "roofline": {"bound": "hbm", "alg_bytes": alg, "plain_frac": alg / plain.seconds / 1e9 / peak,
-                         "batched_frac": alg / bat.seconds / 1e9 / peak, "peak": peak, "peak_kind": peak_kind},
-            "clocks_plain": clk.summary(),
-        })
-        print(json.dumps(row), flush=True)
-    mlp.close()
-
-
+# ------------------------------------------------------------------------------------ arms
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    v, cells, secs = run_oracle(args, args.steps, args.warmup)
-    sample = f"{args.steps} ticks after {args.warmup} warm-up ticks of the workload, oracle port of fluid.rs, 1 thread"
+    w0, nt = args.warmup * TICKS_PER_STEP, args.steps * TICKS_PER_STEP
+    v, cells, secs, _ = oracle_window(args.workload, args.scale, w0, nt)
+    sample = (f"ticks {w0 + 1}..{w0 + nt} after {w0} untimed ticks ({cells} cell-steps), the oracle port of fluid.rs on 1 host thread "
+              "(one world: the reference's sweep is sequential)")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -328,7 +292,7 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism="replicas"),
+        "config": config(args),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -353,11 +317,18 @@ def ours(args):
     stream = torch.cuda.Stream()  # the engine, the L2 flush and the timing events share it
     torch.cuda.set_stream(stream)
     wl = vf.Workload(args.workload, args.scale, 1)
-    world = wl.world(0)
-    sim = vf.FluidSim(world, device=local, stream=stream.cuda_stream)
-    for b in wl.wakes(0):
-        sim.wake(*map(int, b))
-    sim.tick(args.warmup)  # W warm-up steps (whole ticks)
+    w0, nt = args.warmup * TICKS_PER_STEP, args.steps * TICKS_PER_STEP
+
+    def fresh():
+        s = vf.FluidSim(wl.world(0), device=local, stream=stream.cuda_stream)
+        s.set_sweep(args.engine, args.gate)
+        for b in wl.wakes(0):
+            s.wake(*map(int, b))
+        s.tick(w0)  # the untimed steps (whole ticks)
+        return s
+
+    # ---- device-timed: one launch of 10 ticks per step, inputs resident, L2 flushed before each
+    sim = fresh()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     s0 = sim.stats()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -366,16 +337,19 @@ def ours(args):
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         for k in range(args.steps):
-            flush.zero_()  # L2 flushed between timed steps
+            flush.zero_()
             evs[k][0].record(stream)
-            sim.tick_async(1)
+            sim.tick_async(TICKS_PER_STEP)
             evs[k][1].record(stream)
         torch.cuda.synchronize()
     sim.sync()
     if world_size > 1:
         dist.barrier()
     s1 = sim.stats()
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    dig = sim.digest()
+    sim.close()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    dev_ms = sum(step_ms)
     cells = s1.cells_total - s0.cells_total
     lvl = s1.level_cells_total - s0.level_cells_total
     bfs = s1.bfs_visits - s0.bfs_visits
@@ -388,30 +362,28 @@ def ours(args):
     alg_bytes = 10.0 * cells + 5.0 * lvl + 5.0 * bfs
     peak, peak_kind = peaks()
     achieved = alg_bytes / (dev_ms / 1e3) / 1e9
-    # resident variant: all timed ticks in one persistent launch (state stays in L2)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    sA = sim.stats()
-    e0.record(stream)
-    sim.tick_async(args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    sim.sync()
-    sB = sim.stats()
-    resident = (sB.cells_total - sA.cells_total) / (e0.elapsed_time(e1) / 1e3)
-    # end to end through the public API: tick + download of the step's voxel changes + replay
-    # into the host world, host wall time
-    d2h = 0
-    h2d = 0
+    # ---- end to end through the public API, same ticks from the same state: per step the tick
+    # call (control word host->device from pinned memory, the launch, the control block back) and
+    # the download of the step's voxel changes replayed into the host world; host wall time
+    sim = fresh()
+    d2h = h2d = 0
     sC = sim.stats()
+    if world_size > 1:
+        dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        sim.tick(1)
-        n = sim.sync_world()  # download the tick's voxel changes, replay them through set_voxel
-        d2h += 128 + 16 * n + 128  # control block after the tick and after the download, changes
+    for _ in range(args.steps):
+        sim.tick(TICKS_PER_STEP)
+        n = sim.sync_world()
+        d2h += 128 + 16 * n + 128  # control block after the tick and after the download, the changes
         h2d += 4 + 8  # the tick's control word and the download's pending count
     t1 = time.perf_counter()
     sD = sim.stats()
-    e2e = (sD.cells_total - sC.cells_total) / (t1 - t0)
+    e2e_same = sim.digest() == dig
+    sim.close()
+    e2e_secs = torch.tensor([t1 - t0], dtype=torch.float64, device="cuda")
+    if world_size > 1:
+        dist.all_reduce(e2e_secs, op=dist.ReduceOp.MAX)
+    e2e = (sD.cells_total - sC.cells_total) * world_size / float(e2e_secs.item())
     line = {
         "metric": METRIC,
         "value": value,
@@ -425,28 +397,37 @@ def ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world_size}", l2="flushed before every timed step (256 MiB write)",
-                       engine="exact sweep, one warp per region"),
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // max(args.e2e_steps, 1), "d2h_bytes_per_step": d2h // max(args.e2e_steps, 1),
-                "steps": args.e2e_steps, "timer": "host wall clock"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": TICK_DRAM_BYTES,
-                     "peak_kind": peak_kind, "kernel": "k_tick", "alg_bytes_per_step": alg_bytes / args.steps},
-        "resident_value": resident,
+        "config": config(args),
+        "engine": {"engine": args.engine, "gate": args.gate,
+                   "sweep": "parallel exact sweep, rows on 16 warps of one CTA" if args.engine else "one-warp exact sweep + 7 prefetching warps"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // max(args.steps, 1), "d2h_bytes_per_step": d2h // max(args.steps, 1),
+                "steps": args.steps, "timer": "host wall clock", "same_ticks_as_value": True, "same_end_state": bool(e2e_same)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": STEP_DRAM_BYTES,
+                     "traffic_source": "one-off ncu capture of one step's k_tick_par launch (dram__bytes read + write)",
+                     "peak_kind": peak_kind, "kernel": "k_tick_par" if args.engine else "k_tick", "alg_bytes_per_step": alg_bytes / args.steps},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "cells_per_step": cells / args.steps,
+        "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
     }
-    if rank == 0 and not args.no_variants:
-        line["variants"] = variants(args, vf, wl, torch, stream)
     if rank == 0 and not args.no_cpu_baseline:
-        ticks = max(args.steps, CPU_SAMPLE_TICKS)
-        runs = [run_oracle(args, ticks, args.warmup) for _ in range(3)]
-        v, c, secs = sorted(runs)[1]
+        v, c, secs, odig = oracle_window(args.workload, args.scale, w0, nt, reps=3)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"ticks {args.warmup}..{args.warmup + ticks} of the workload ({c} cell-steps, {secs:.2f} s), median of 3 runs, oracle port of fluid.rs, 1 thread"}
+                                "sample": f"ticks {w0 + 1}..{w0 + nt} ({c} cell-steps, {secs:.2f} s), median of 3 runs, oracle port of fluid.rs, 1 thread"}
+        line["oracle_digest_match"] = odig == dig
+    if rank == 0 and not args.no_variants:
+        from vfwater import proposal
+
+        mlp, info = proposal.train_default(vf, torch)
+        v = headline_variants(vf, torch, stream, args, mlp)
+        v["learned"].update({"heldout": info["heldout"], "persistence": info["persistence"]})
+        threads = os.cpu_count() or 1
+        for wid, desc in VARIANTS:
+            v[f"config{wid}"] = variant_row(vf, torch, stream, wid, desc, args.variant_ticks, mlp, threads)
+        mlp.close()
+        line["variants"] = v
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sim.close()
     if world_size > 1:
         dist.destroy_process_group()
 
@@ -455,8 +436,6 @@ def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
-    elif args.suite:
-        suite(args)
     else:
         ours(args)
 

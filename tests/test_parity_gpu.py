@@ -357,9 +357,9 @@ def test_autotuner_times_candidates_and_caches_the_best(vf, tmp_path, monkeypatc
     from vfwater import autotune
 
     monkeypatch.setattr(autotune, "CACHE", tmp_path / "tune.json")
-    cands = [{"producers": 2, "depth": 8, "ticks_per_launch": 4}, {"producers": 7, "depth": 64, "ticks_per_launch": 4}]
+    cands = [{"engine": 0, "producers": 2, "depth": 8, "ticks_per_launch": 4}, {"engine": 1, "gate": 2, "ticks_per_launch": 4}]
     best, table = autotune.tune(vf, 3, 0.1, torch, warmup=2, ticks=4, candidates=cands, seed=4)
-    assert best in [{k: c[k] for k in autotune.DEFAULT} for c in cands]
+    assert best in [dict(autotune.DEFAULT, **c) for c in cands]
     assert len(table) == 2 and all(r["cell_steps_per_s"] > 0 for r in table)
     cache = json.loads((tmp_path / "tune.json").read_text())
     (key, entry), = cache.items()

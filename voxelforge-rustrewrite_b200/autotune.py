@@ -1,8 +1,11 @@
 """Autotuner for the tick's launch knobs.
 
 The knobs change how fast a tick runs, never what it computes (every setting is bit-exact):
-  * producers - warps that prefetch upcoming cells' footprints into the shared-memory ring (1..7)
-  * depth     - how many cells ahead of the sweep they may run (1..64)
+  * engine    - 0: the one-warp sweep with prefetching warps (256 threads per region);
+                1: the parallel sweep, rows of the sorted order on 16 warps (512 threads per region)
+  * gate      - engine 1: the pull gate / lower-layer cone radius in cells (the schedule's shape)
+  * producers - engine 0: warps that prefetch upcoming cells' footprints into the shared-memory ring
+  * depth     - engine 0: how many cells ahead of the sweep they may run (1..64)
   * ticks_per_launch - ticks one persistent launch runs before returning to the host
 
 A candidate is timed on fresh copies of the workload's regions: `warmup` ticks with the default
@@ -15,8 +18,15 @@ import json
 import os
 from pathlib import Path
 
-DEFAULT = {"producers": 7, "depth": 64, "ticks_per_launch": 10}
-CANDIDATES = [{"producers": p, "depth": d, "ticks_per_launch": 10} for p in (1, 2, 4, 7) for d in (16, 64)]
+DEFAULT = {"engine": 1, "gate": 4, "producers": 7, "depth": 64, "ticks_per_launch": 10}
+CANDIDATES = [dict(DEFAULT, engine=0, producers=p, depth=d) for p in (2, 7) for d in (16, 64)] + [dict(DEFAULT, gate=g) for g in (2, 4, 8)]
+
+
+def apply(sim, knobs: dict):
+    """Set a candidate's knobs on one handle (missing keys take DEFAULT's)."""
+    k = dict(DEFAULT, **knobs)
+    sim.set_sweep(k["engine"], k["gate"])
+    sim.set_tuning(k["producers"], k["depth"])
 CACHE = Path(os.environ.get("VF_TUNE_CACHE", Path(__file__).resolve().parent / "autotune_cache.json"))
 
 
@@ -61,7 +71,7 @@ def tune(vf, wid: int, scale: float, torch, warmup: int = 10, ticks: int = 20, c
         batch.tick_async(warmup)
         batch.sync()
         for s in sims:
-            s.set_tuning(cand["producers"], cand["depth"])
+            apply(s, cand)
         batch.close()
         batch = vf.Batch(sims)  # region table re-read with the new knobs
         c0 = sum(s.stats().cells_total for s in sims)
@@ -69,7 +79,7 @@ def tune(vf, wid: int, scale: float, torch, warmup: int = 10, ticks: int = 20, c
         e0.record(stream)
         left = ticks
         while left > 0:
-            n = min(left, cand["ticks_per_launch"])
+            n = min(left, dict(DEFAULT, **cand)["ticks_per_launch"])
             batch.tick_async(n)
             left -= n
         e1.record(stream)
@@ -77,13 +87,14 @@ def tune(vf, wid: int, scale: float, torch, warmup: int = 10, ticks: int = 20, c
         batch.sync()
         cells = sum(s.stats().cells_total for s in sims) - c0
         secs = e0.elapsed_time(e1) / 1e3
-        table.append(dict(cand, cell_steps_per_s=cells / secs if secs else 0.0, cells=cells, seconds=secs))
+        table.append(dict(DEFAULT, **cand, cell_steps_per_s=cells / secs if secs else 0.0, cells=cells, seconds=secs))
         batch.close()
         for s in sims:
             s.close()
     best = max(table, key=lambda r: r["cell_steps_per_s"])
     cells_total = wl.resident_cells
     c = load_cache()
-    c[_key(gpu, wid, cells_total)] = {"best": {k: best[k] for k in DEFAULT}, "table": table, "scale": scale}
+    knobs = {k: dict(DEFAULT, **best)[k] for k in DEFAULT}
+    c[_key(gpu, wid, cells_total)] = {"best": knobs, "table": table, "scale": scale}
     save_cache(c)
-    return {k: best[k] for k in DEFAULT}, table
+    return knobs, table

@@ -34,12 +34,15 @@ class RunResult:
 
 
 def make_sims(vf, wl, stream_handle: int, regions=None, tune=None):
-    """One FluidSim per region (all on one stream), initial wake boxes applied."""
+    """One FluidSim per region (all on one stream), initial wake boxes applied. `tune`: a dict of
+    autotune knobs (engine, gate, producers, depth)."""
+    from . import autotune
+
     sims = []
     for r in (range(wl.regions) if regions is None else regions):
         sim = vf.FluidSim(wl.world(r), stream=stream_handle)
         if tune:
-            sim.set_tuning(*tune)
+            autotune.apply(sim, tune)
         for b in wl.wakes(r):
             sim.wake(*map(int, b))
         sims.append(sim)
