@@ -204,17 +204,24 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
  * gate: bits 0-7 (0..31, default 4) before a pressure search, wait for the earlier cells of its layer
  * within this Chebyshev distance; bits 8-15 (0..31, 0 = the same value) a cell of a segment with
  * pulls starts only when rows in work on lower layers within that many rows have passed its x plus
- * that distance (fewer replays, less overlap). spin_cap (> 0, default 2^24): iterations
- * of a device wait before the tick gives up with VF_ERR_TIMEOUT.
+ * that distance (fewer replays, less overlap). spin_cap (> 0, default 2^24): iterations of any device
+ * wait (both engines, and the levelling's brick materialisation) before the tick gives up with
+ * VF_ERR_TIMEOUT; the kernel then returns and the handle can only be destroyed.
  * No reference counterpart: a device scheduling knob of this library. */
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap);
 
 /* Parallel-sweep counters summed over ticks: budget segments run, segments undone and replayed in
  * sorted order, cells replayed, and (conflicts3, 3 entries, optional) the conflicts that caused the
- * replays: a later reader of a pull's source had started, a later pull had read the source, the
- * source would have joined the cells that may attempt a pull. No reference counterpart
- * (diagnostics). */
+ * replays: a later reader of a pull's source had started, a later pull had read the source, more
+ * cells of a segment attempted a pull than the tick's budget had left (cells that earlier pulls
+ * took below full). No reference counterpart (diagnostics). */
 int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3);
+
+/* Lower the per-tick event-log capacities (activations, level seeds, voxel changes; each 1 .. its
+ * allocated size, 2^22 / 2^18 / 2^21). A tick whose events overflow a log fails with VF_ERR_OOM
+ * (the state is then undefined). The allocated sizes hold any tick (at most 50,000 drained cells);
+ * lower values serve tests of the overflow path. No reference counterpart. */
+int vf_fluid_set_log_caps(vf_fluid* h, uint32_t act, uint32_t seed, uint32_t chg);
 
 /* Parallel-sweep SM cycle counters summed over ticks (18 entries): prepass, segments, rollbacks,
  * event logs; then summed over warps: dependency waits, blocked starts, footprint loads, pulls,

@@ -55,6 +55,10 @@ void vf_world_compact(vf_world* w);
 /* Ring paste / evict (sparse_volume.rs:478-537). */
 int vf_world_ring_paste(vf_world* ring, const vf_world* chunk, int32_t cx, int32_t cz);
 int vf_world_ring_evict(vf_world* ring, int32_t cx, int32_t cz);
+/* SparseVolume::ring_rebase (sparse_volume.rs:194-203): the floating origin moves by (dcx, dcz)
+ * chunks; every slot's owner moves, the bricks stay. Pair it with vf_fluid_shift(dcx * 128,
+ * dcz * 128) on the handles simulating this world. */
+int vf_world_ring_rebase(vf_world* ring, int32_t dcx, int32_t dcz);
 int vf_world_chunk_loaded(const vf_world* w, int32_t cx, int32_t cz);
 
 /* Raw views of the grid (bricks_x*bricks_y*bricks_z u32), the brick pool (nbricks*512 u8) and

@@ -39,6 +39,16 @@ bool SparseVolume::chunk_loaded(int32_t cx, int32_t cz) const {  // :164-170
   return s.loaded && s.cx == cx && s.cz == cz;
 }
 
+// The floating origin moves by (dcx, dcz) chunks: every slot's owner moves, the bricks stay.
+void SparseVolume::ring_rebase(int32_t dcx, int32_t dcz) {  // :194-203
+  for (auto& s : ring_slots) {
+    s.cx -= dcx;
+    s.cz -= dcz;
+  }
+  origin_x += dcx * RING_CHUNK_B * BRICK;
+  origin_z += dcz * RING_CHUNK_B * BRICK;
+}
+
 bool SparseVolume::loaded_at(int32_t x, int32_t z) const {  // :173-175
   return ring_w == 0 || chunk_loaded(x >> 7, z >> 7);
 }

@@ -166,6 +166,7 @@ struct SparseVolume {
   bool chunk_loaded(int32_t cx, int32_t cz) const;                   // :164-170
   bool loaded_at(int32_t x, int32_t z) const;                        // :173-175
   void ring_init(int32_t w, int32_t ny);                             // :177-192
+  void ring_rebase(int32_t dcx, int32_t dcz);                        // :194-203
   bool inside(int32_t x, int32_t y, int32_t z) const;                // :229-235
   uint8_t get_voxel(int32_t x, int32_t y, int32_t z) const;          // :238-247
   size_t materialize(size_t gi, uint8_t fill);                       // :250-266

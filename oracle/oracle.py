@@ -56,6 +56,7 @@ def lib():
         "orc_volume": (C.c_float, [P, I32, I32, I32]),
         "orc_set_partial": (None, [P, I32, I32, I32, C.c_float]),
         "orc_shift": (None, [P, I32, I32]),
+        "orc_ring_rebase": (None, [P, I32, I32]),
         "orc_reset": (None, [P]),
         "orc_idle": (C.c_int, [P]),
         "orc_active_count": (C.c_uint64, [P]),
@@ -166,6 +167,10 @@ class Oracle:
 
     def shift(self, dx, dz):
         lib().orc_shift(self.h, dx, dz)
+
+    def ring_rebase(self, dcx, dcz):
+        """SparseVolume::ring_rebase: the floating origin moves by (dcx, dcz) chunks."""
+        lib().orc_ring_rebase(self.h, dcx, dcz)
 
     def reset(self):
         lib().orc_reset(self.h)

@@ -86,6 +86,7 @@ uint64_t orc_apply_brush(orc_handle* h, const int32_t* xyz, uint64_t n, uint8_t 
 float orc_volume(orc_handle* h, int32_t x, int32_t y, int32_t z) { return h->s.volume(h->v, x, y, z); }
 void orc_set_partial(orc_handle* h, int32_t x, int32_t y, int32_t z, float val) { h->s.set_partial(x, y, z, val); }
 void orc_shift(orc_handle* h, int32_t dx, int32_t dz) { h->s.shift(dx, dz); }
+void orc_ring_rebase(orc_handle* h, int32_t dcx, int32_t dcz) { h->v.ring_rebase(dcx, dcz); }
 void orc_reset(orc_handle* h) { h->s.reset(); }
 int orc_idle(orc_handle* h) { return h->s.idle() ? 1 : 0; }
 uint64_t orc_active_count(orc_handle* h) { return h->s.active_count(); }

@@ -111,6 +111,7 @@ def lib():
         "vf_world_compact": (None, [P]),
         "vf_world_ring_paste": (C.c_int, [P, P, I32, I32]),
         "vf_world_ring_evict": (C.c_int, [P, I32, I32]),
+        "vf_world_ring_rebase": (C.c_int, [P, I32, I32]),
         "vf_world_chunk_loaded": (C.c_int, [P, I32, I32]),
         "vf_world_grid": (C.POINTER(C.c_uint32), [P]),
         "vf_world_bricks": (C.POINTER(C.c_uint8), [P]),
@@ -154,6 +155,7 @@ def lib():
         "vf_fluid_batch_tick": (C.c_int, [C.POINTER(P), I32, I32]),
         "vf_fluid_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_set_tuning": (C.c_int, [P, I32, I32]),
+        "vf_fluid_set_log_caps": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32]),
         "vf_fluid_set_sweep": (C.c_int, [P, I32, I32, C.c_uint64]),
         "vf_fluid_sweep_profile": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "vf_fluid_sweep_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
@@ -245,6 +247,10 @@ class World:
 
     def ring_evict(self, cx: int, cz: int):
         lib().vf_world_ring_evict(self.h, cx, cz)
+
+    def ring_rebase(self, dcx: int, dcz: int):
+        """SparseVolume::ring_rebase: the floating origin moves by (dcx, dcz) chunks."""
+        lib().vf_world_ring_rebase(self.h, dcx, dcz)
 
     def chunk_loaded(self, cx, cz) -> bool:
         return bool(lib().vf_world_chunk_loaded(self.h, cx, cz))
@@ -386,6 +392,10 @@ class FluidSim:
         """Which sweep runs (0 one warp, 1 all warps of the region's CTA), the parallel sweep's pull
         gate radius and the iteration cap of device waits; results never depend on them."""
         self._check(lib().vf_fluid_set_sweep(self.h, engine, gate, spin_cap), "set_sweep")
+
+    def set_log_caps(self, act: int, seed: int, chg: int):
+        """Lower the per-tick event-log capacities (a tick that overflows one fails with VF_ERR_OOM)."""
+        self._check(lib().vf_fluid_set_log_caps(self.h, act, seed, chg), "set_log_caps")
 
     SWEEP_PROFILE = ("prepass", "segments", "rollbacks", "logs", "dep_wait", "start_wait", "footprint", "pulls", "writes", "cells",
                      "row_fetch", "worker_total", "cone_wait", "gate_wait", "searches", "rounds", "search_reads",

@@ -932,6 +932,20 @@ int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_
   return VF_OK;
 }
 
+int vf_fluid_set_log_caps(vf_fluid* h, uint32_t act, uint32_t seed, uint32_t chg) {
+  int rc = check(h);
+  if (rc) return rc;
+  if (act < 1 || act > (1u << 22) || seed < 1 || seed > (1u << 18) || chg < 1 || chg > (1u << 21)) return VF_ERR_INVALID;
+  DeviceScope scope(h->device);
+  if (scope.err != cudaSuccess) return VF_ERR_CUDA;
+  if ((rc = sync_ctl(h))) return rc;
+  h->R.ev_act_cap = act;
+  h->R.ev_seed_cap = seed;
+  h->R.ev_chg_cap = chg;
+  CK(cudaMemcpyAsync(h->dR, &h->R, sizeof(Region), cudaMemcpyHostToDevice, h->stream));
+  return sync_ctl(h);
+}
+
 int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out18) {
   int rc = check(h);
   if (rc) return rc;

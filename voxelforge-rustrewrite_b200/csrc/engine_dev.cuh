@@ -151,7 +151,6 @@ constexpr unsigned EMPTY_ID = 0xFFFFFFFFu;
 // never waits for a helper. Before a new search begins, the old one closes its state and waits
 // (bounded) until no helper is in flight, so no helper of an old search writes a slot again.
 constexpr unsigned HRING = 64;
-constexpr unsigned long long HELP_WAIT_CAP = 1ull << 23;  // bounded wait for helpers in flight
 struct SearchHelp {
   CD nb[HRING][5];                // neighbours (up, +x, -x, +z, -z) of entry q at slot q % HRING
   unsigned long long tag[HRING];  // epoch << 32 | q once nb[q % HRING] is complete
@@ -170,6 +169,8 @@ struct Smem {
   unsigned* vb;             // VB_WORDS: visited bitmap of the search box (all zero between searches)
   unsigned* vtl;            // PRESS_QCAP: bitmap words the current search set (cleared at its end)
   SearchHelp* help;         // neighbour loads ahead of the search (null: none)
+  unsigned* abort;          // the one-warp sweep's stop flag (null outside it)
+  unsigned long long spin_cap;  // iterations before a wait on the helpers gives up (ST_TIMEOUT)
 };
 
 __device__ __forceinline__ void set_status(const Region& R, int st, unsigned info) {
@@ -730,13 +731,16 @@ __device__ float pressure_pull(const Region& R, WS& W, Smem& S, ActList& A, int 
       }
       unsigned long long spins = 0;
       while ((*(volatile unsigned long long*)&H->state & 0xFFFFFull) != 0ull) {
-        if (++spins > HELP_WAIT_CAP) {
+        if (++spins > S.spin_cap) {
           ok2 = 0u;
           break;
         }
         __nanosleep(20);
       }
-      if (!ok2) set_status(R, ST_TIMEOUT, 21);
+      if (!ok2) {  // the sweep stops: no new search may reuse the ring while a helper runs
+        set_status(R, ST_TIMEOUT, 21);
+        if (S.abort) *(volatile unsigned*)S.abort = 1u;
+      }
       __threadfence_block();
     }
     __syncwarp();

@@ -143,8 +143,6 @@ struct Tune {
   int gate;       // parallel sweep: 0 .. GATE_MAX
   unsigned long long spin_cap;  // iterations before a wait gives up (ST_TIMEOUT)
 };
-constexpr unsigned long long SPIN_CAP = 1ull << 24; // bounded waits (~seconds), then an error status
-constexpr unsigned long long SPIN_CAP_SLEEP = 1ull << 23;  // waits with a nanosleep per round
 
 // Shared memory of the one-warp sweep: prefetch ring, store forwarding and search structures.
 struct SeqSmem {
@@ -402,7 +400,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
     WS W = sW;
     W.fwd = sm.u.s.fwd;
     W.gc = sm.u.s.gc;
-    Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, &sm.u.s.help};
+    Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, &sm.u.s.help, &sm.u.s.abort, tune.spin_cap};
     const unsigned pxy = (unsigned)R.PX * (unsigned)R.PY;
     // footprint offsets (self, below, up, +x, -x, +z, -z) of this lane, in cells and in ids
     const int ox = (lane == 3) - (lane == 4), oy = (lane == 2) - (lane == 1), oz = (lane == 5) - (lane == 6);
@@ -413,10 +411,10 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       const long long tw = fine_clock();
       unsigned long long spins = 0;
       while (*(volatile unsigned*)&sm.u.s.pf_ready[slot] != r) {
-        if (++spins > SPIN_CAP_SLEEP) break;
+        if (++spins > tune.spin_cap) break;
         __nanosleep(20);
       }
-      if (spins > SPIN_CAP_SLEEP) {
+      if (spins > tune.spin_cap) {
         if (lane == 0) {
           set_status(R, ST_TIMEOUT, 20);
           *(volatile unsigned*)&sm.u.s.abort = 1u;
@@ -518,7 +516,7 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
       unsigned c0;
       bool ok = true;
       while ((c0 = *(volatile unsigned*)&sm.u.s.consumed) + depth <= r) {
-        if (*(volatile unsigned*)&sm.u.s.abort || ++spins > SPIN_CAP_SLEEP) {
+        if (*(volatile unsigned*)&sm.u.s.abort || ++spins > tune.spin_cap) {
           ok = false;
           break;
         }
@@ -1436,7 +1434,7 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
     if (tid == 0) s_lv = (sW.level_round || (R.ctl->tick_no % LEVEL_TICKS) == 0u) ? 1u : 0u;
     __syncthreads();
     if (s_lv) {
-      Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, nullptr};
+      Smem S{sm.u.s.vis, ring, sm.u.s.pq, sm.u.s.vb, sm.u.s.vtl, nullptr, nullptr, tune.spin_cap};
       if (tid == 0) sW.llc = 0;
       __syncthreads();
       level_round_cta(R, sm, sW, S, tune.spin_cap);

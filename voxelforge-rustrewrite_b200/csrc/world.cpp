@@ -476,6 +476,16 @@ int vf_world_ring_evict(vf_world* ring, int32_t cx, int32_t cz) {
   ring->w.ring_evict(cx, cz);
   return VF_OK;
 }
+int vf_world_ring_rebase(vf_world* ring, int32_t dcx, int32_t dcz) {  // sparse_volume.rs:194-203
+  if (!ring || ring->w.ring_w == 0) return VF_ERR_INVALID;
+  for (RingSlot& s : ring->w.ring_slots) {
+    s.cx -= dcx;
+    s.cz -= dcz;
+  }
+  ring->w.origin_x += dcx * 128;
+  ring->w.origin_z += dcz * 128;
+  return VF_OK;
+}
 int vf_world_chunk_loaded(const vf_world* w, int32_t cx, int32_t cz) { return w->w.chunk_loaded(cx, cz) ? 1 : 0; }
 const uint32_t* vf_world_grid(const vf_world* w) { return w->w.grid.data(); }
 const uint8_t* vf_world_bricks(const vf_world* w) { return w->w.bricks.empty() ? nullptr : w->w.bricks[0].data(); }

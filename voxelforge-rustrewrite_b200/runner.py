@@ -57,10 +57,11 @@ def _emits_before(wl, t):
     return bool(wl.emit_every) and (t % wl.emit_every) == 0
 
 
-def run_plain(vf, wl, sims, t0: int, ticks: int, torch, stream) -> RunResult:
-    """Host-driven baseline: per tick, per region: edits, then one tick with a host sync."""
-    regions = list(range(len(sims)))
-    emitters = [wl.emitters(r) for r in regions]
+def run_plain(vf, wl, sims, t0: int, ticks: int, torch, stream, regions=None) -> RunResult:
+    """Host-driven baseline: per tick, per region: edits, then one tick with a host sync.
+    `regions`: the workload regions the sims hold (default 0..len(sims)-1)."""
+    regions = list(range(len(sims))) if regions is None else list(regions)
+    emitters = {r: wl.emitters(r) for r in regions}
     c0 = [s.stats().cells_total for s in sims]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
