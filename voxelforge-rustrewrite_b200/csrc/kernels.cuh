@@ -735,7 +735,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
       if (warp == 0) {
         unsigned sp = s_c;
         unsigned cgi = 0xFFFFFFFFu, cg = 0u;
-        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf, NOSLOT, cgi, cg);
+        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf, NOSLOT, cgi, cg, NOSLOT, 0u);
         if (lane == 0) R.ctl->par_replayed += T.seg_end - T.seg_start;
       }
       __syncthreads();
@@ -749,7 +749,8 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
         if (lane == 0) t = atomicAdd(&ps.next_task, 1u);
         t = __shfl_sync(FULLMASK, t, 0);
         if (t > ps.task_end) break;
-        const unsigned a = max(R.rowstart[t], T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
+        const unsigned rs = R.rowstart[t];
+        const unsigned a = max(rs, T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
         // publish the row and its next cell for cone_wait (key / PX = y * PZ + sorted z)
         const unsigned ka = R.cells[a];
         const unsigned yz = ka / (unsigned)R.PX, yy = yz / (unsigned)R.PZ, zs = yz - yy * (unsigned)R.PZ;
@@ -763,7 +764,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
           const unsigned jr = jr_next;
           if (i + 1u < b) jr_next = R.deps[(i + 1u) * 16u + (lane & 15u)];  // used by the next cell
           if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = rowtag | (R.cells[i] - yz * (unsigned)R.PX);
-          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf, jr, cgi, cg);
+          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf, jr, cgi, cg, t, rs);
         }
         if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = WROW_IDLE;
         if (!ok || vld(&ps.abort)) break;

@@ -801,9 +801,11 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
 // running beside other warps (waits, blocking, multi-version pull reads); PM_SEQ: one warp replaying
 // a segment in order, attempts counted in `seq_pulls`. Returns false when the segment stops.
 // jr: this lane's entry of the cell's earlier conflicting cells (ParDeps, lanes 0..9); cgi / cg:
-// the lane's grid-word cache (load_cell_cached).
+// the lane's grid-word cache (load_cell_cached); row / rstart: the cell's row and its first sorted
+// position (row NOSLOT: looked up).
 __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* ring, const ParTick& T, int mode, unsigned i,
-                                 unsigned& seq_pulls, ParProf& pf, unsigned jr, unsigned& cgi, unsigned& cg) {
+                                 unsigned& seq_pulls, ParProf& pf, unsigned jr, unsigned& cgi, unsigned& cg, unsigned row,
+                                 unsigned rstart) {
   const unsigned lane = lane_id();
   long long c0 = clock64();
   const float FULL = full_level();
@@ -886,7 +888,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   bool live = true;
   if (cd_solid(fp[0])) {
     // fluid.rs:586-589: a solid cell's partial entry is erased
-    w = lane == 0 && fp[0].slot != NOSLOT && fp[0].part > 0.0f;
+    w = lane == 0 && mine.slot != NOSLOT && mine.part > 0.0f;
     live = false;
   }
   float vol = cd_volume(fp[0]);
@@ -963,8 +965,8 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   }
   const unsigned wmask = __ballot_sync(FULLMASK, w) & 0x7Fu;
   const unsigned chm = __ballot_sync(FULLMASK, w && p.ch) & 0x7Fu;
-  int pd = w ? p.dp : 0;
-  for (int o = 16; o; o >>= 1) pd += __shfl_xor_sync(FULLMASK, pd, o);
+  // partial-entry count change: each lane's is -1, 0 or +1
+  const int pd = __popc(__ballot_sync(FULLMASK, w && p.dp > 0)) - __popc(__ballot_sync(FULLMASK, w && p.dp < 0));
   if (lane == 0) {
     co.cmask |= chm;
     co.pdelta += pd;
@@ -990,8 +992,11 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   __syncwarp();
   __threadfence_block();
   if (lane == 0) {
-    const unsigned r = R.rowof[i] & 0x3FFFFFFFu;
-    vst(R.rowprog + r, i - R.rowstart[r] + 1u);
+    if (row == NOSLOT) {
+      row = R.rowof[i] & 0x3FFFFFFFu;
+      rstart = R.rowstart[row];
+    }
+    vst(R.rowprog + row, i - rstart + 1u);
     if (mode != PM_SEQ) cs_advance(ps.state, i);
     else ps.state[i >> 2] = (ps.state[i >> 2] & ~(0xFFu << sh)) | (CS_DONE << sh);
   }
