@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--workload", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--engine", type=int, default=1, help="0: one-warp sweep, 1: parallel sweep")
-    ap.add_argument("--gate", type=int, default=4)
+    ap.add_argument("--gate", type=int, default=4 | (1 << 8), help="same-layer gate | lower-layer cone << 8")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--variant-ticks", type=int, default=100)
@@ -191,7 +191,7 @@ VARIANTS = [
     (4, "ring 9x9 chunks of 128x256x128 (1152x256x1152), sea y<64, 1000 rain emitters, 1 level per 4 ticks"),
 ]
 VARIANT_TUNE = [{"engine": 0, "producers": 7, "depth": 64, "ticks_per_launch": 10}, {"engine": 1, "gate": 4, "ticks_per_launch": 10},
-                {"engine": 1, "gate": 8, "ticks_per_launch": 10}]
+                {"engine": 1, "gate": 4 | (1 << 8), "ticks_per_launch": 10}]
 
 
 def _digests(sims):

@@ -202,7 +202,7 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
  * cell waiting for the earlier cells it conflicts with; pressure searches read cells as of their own
  * position; a segment whose order the schedule cannot keep is undone and replayed by one warp.
  * gate: bits 0-7 (0..31, default 4) before a pressure search, wait for the earlier cells of its layer
- * within this Chebyshev distance; bits 8-15 (0..31, 0 = the same value) a cell of a segment with
+ * within this Chebyshev distance; bits 8-15 (0..31, 0 = the same value, default 1) a cell of a segment with
  * pulls starts only when rows in work on lower layers within that many rows have passed its x plus
  * that distance (fewer replays, less overlap). spin_cap (> 0, default 2^24): iterations of any device
  * wait (both engines, and the levelling's brick materialisation) before the tick gives up with

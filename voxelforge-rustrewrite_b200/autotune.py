@@ -18,8 +18,8 @@ import json
 import os
 from pathlib import Path
 
-DEFAULT = {"engine": 1, "gate": 4, "producers": 7, "depth": 64, "ticks_per_launch": 10}
-CANDIDATES = [dict(DEFAULT, engine=0, producers=p, depth=d) for p in (2, 7) for d in (16, 64)] + [dict(DEFAULT, gate=g) for g in (2, 4, 8)]
+DEFAULT = {"engine": 1, "gate": 4 | (1 << 8), "producers": 7, "depth": 64, "ticks_per_launch": 10}
+CANDIDATES = [dict(DEFAULT, engine=0, producers=p, depth=d) for p in (2, 7) for d in (16, 64)] + [dict(DEFAULT, gate=g) for g in (2, 4, 4 | (1 << 8), 8)]
 
 
 def apply(sim, knobs: dict):

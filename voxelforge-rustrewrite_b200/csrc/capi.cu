@@ -34,7 +34,7 @@ struct vf_fluid {
   size_t scratch_bytes = 0;
   // tick launch shape
   int smem_bytes = 0;
-  Tune tune{TICK_WARPS - 1, PF_RING, 1, 4, 1ull << 24};
+  Tune tune{TICK_WARPS - 1, PF_RING, 1, 4 | (1 << 8), 1ull << 24};
   // wake proposal state (allocated on first use)
   int* slot_gi = nullptr;
   SlotAggr* aggr = nullptr;

@@ -58,12 +58,13 @@ struct Ctl {
   unsigned int seg_epoch;           // parallel sweep: segments begun so far (tags versions and reads)
   unsigned int ptn;                 // parallel sweep: cells listed in Region::ptlist this tick
   unsigned int pxn;                 // parallel sweep: positions listed in Region::pxlist this tick
-  unsigned int pad2;
+  unsigned int att_ratio;           // parallel sweep: pull attempts per possible attempter of the
+                                    // last tick's completed segments, x 65536 (0: none yet)
   // parallel sweep diagnostics, summed over ticks: budget segments run, segments rolled back and
   // replayed in order by one warp, cells replayed
   unsigned long long par_segments, par_rollbacks, par_replayed;
   // conflicts by kind: a later reader of a pull's source had started, a later pull had read the
-  // source, the source would join the cells that may attempt a pull
+  // source, more cells of a segment attempted a pull than the budget had left
   unsigned long long par_conflicts[4];
   // parallel sweep cycle counters: 0 prepass, 1 segments (workers), 2 rollbacks, 3 event logs;
   // summed over warps: 4 dependency waits, 5 start (blocked), 6 footprint loads, 7 pulls (gate and

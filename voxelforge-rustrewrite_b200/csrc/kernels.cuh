@@ -557,9 +557,13 @@ __device__ void sweep(const Region& R, TickSmem& sm, WS& sW, const int* ring, un
 // Segment end for `room` more attempts from `pos` (one thread): the largest e <= n with at most
 // `room` cells in [pos, e) that may attempt a pull. `extra` cells at or after pos, taken below full
 // by earlier pulls of the tick although not counted in pcnt, are charged up front.
-__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room, unsigned extra) {
+__device__ unsigned seg_end_for(const Region& R, unsigned pos, unsigned n, unsigned room, unsigned extra, float ratio, float factor) {
   if (extra >= room) return pos + 1u;
-  const unsigned lim = R.pcnt[pos] + room - extra;
+  // sized for `factor` times the attempts expected at `ratio` per possible attempter; a segment
+  // that overshoots the budget is undone and cut at its room-th attempt (exact either way)
+  unsigned span = room - extra;
+  if (span > 32u && ratio * (1.0f / factor) < 1.0f) span = (unsigned)fminf(4.0e9f, factor * (float)span / ratio);
+  const unsigned lim = R.pcnt[pos] + span;
   unsigned lo = pos + 1u, hi = n;  // answer in [pos + 1, n]
   while (lo < hi) {
     const unsigned m = (lo + hi + 1u) >> 1;
@@ -681,6 +685,16 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
   const int gate = max(0, min(tune.gate & 0xFF, GATE_MAX));
   const int cone = tune.gate >> 8 ? max(0, min((tune.gate >> 8) & 0xFF, GATE_MAX)) : gate;
   __shared__ unsigned s_extra;
+  // attempts per possible attempter over this tick's completed pull segments (the last tick's to
+  // start with), for sizing the next segment
+  __shared__ unsigned long long s_att_acc, s_p_acc;
+  __shared__ unsigned s_pull_end, s_nseg;
+  if (tid == 0) {
+    s_att_acc = 0ull;
+    s_p_acc = 0ull;
+    s_pull_end = n;  // known once a segment overshot the budget: its room-th attempt's cell + 1
+    s_nseg = 0;
+  }
   while (true) {
     // cells at or after the position that earlier pulls took below full (not counted in pcnt)
     {
@@ -698,7 +712,15 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
           s_end = n;
           s_mode = PM_NOPULL;
         } else {
-          s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c, s_extra);
+          float ratio = 1.0f;
+          if (s_p_acc >= 256ull) ratio = (float)s_att_acc / (float)s_p_acc;
+          else if (R.ctl->att_ratio) ratio = (float)R.ctl->att_ratio * (1.0f / 65536.0f);
+          ratio = fminf(1.0f, fmaxf(ratio, 0.125f));
+          // the tick's first segment stops short of the expected budget end; later ones reach past
+          // it, so that an overshoot finds the exact end, after which one segment runs the rest
+          // with pulls up to that end and none after it
+          if (s_pull_end < n) s_end = n;
+          else s_end = seg_end_for(R, pos, n, MAX_PULLS_PER_TICK - s_c, s_extra, ratio, s_nseg == 0u ? 0.9f : 1.25f);
           s_mode = PM_PULL;
         }
         s_end = min(s_end, max(s_cap, pos + 1u));
@@ -723,6 +745,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
     ParTick T;
     T.seg_start = s_pos;
     T.seg_end = s_end;
+    T.pull_end = s_pull_end;
     T.epoch = s_epoch;
     T.gate = gate;
     T.cone = cone;
@@ -828,12 +851,18 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
       if (tid == 0) {
         R.ctl->par_rollbacks += 1ull;
         R.ctl->par_conflicts[2] += 1ull;
-        s_cap = s_cut;
+        s_pull_end = s_cut;
+        s_cap = n;
       }
       __syncthreads();
       continue;
     }
     if (tid == 0) {
+      if (mode == PM_PULL) {
+        s_att_acc += att;
+        s_p_acc += R.pcnt[min(T.seg_end, T.pull_end)] - R.pcnt[T.seg_start];
+        s_nseg += 1u;
+      }
       s_c += (unsigned)att;
       s_pos = T.seg_end;
       s_cap = n;
@@ -841,6 +870,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
     }
     __syncthreads();
   }
+  if (tid == 0 && s_p_acc >= 256ull) R.ctl->att_ratio = (unsigned)(65536.0 * (double)s_att_acc / (double)s_p_acc);
   if (lane == 0) {
     unsigned long long* q = R.ctl->pprof;
     atomicAdd(q + 4, pf.dep);
@@ -1227,7 +1257,7 @@ __device__ __noinline__ void level_finish_cta(const Region& R, TickSmem& sm, WS&
 // marked (a start that is not a member is marked, and skipped by every later flood fill, either
 // way). sW.level_round is updated at the end.
 __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& sW, Smem& S, unsigned long long cap) {
-  __shared__ unsigned s_ns, s_stop, s_brk, s_pend, s_qi, s_ql;
+  __shared__ unsigned s_ns, s_stop, s_brk, s_pend, s_qi, s_ql, s_cur;
   const unsigned tid = threadIdx.x;
   unsigned* b_start = sm.hist;          // the batch's starts (domain ids), by seed
   unsigned* b_cand = sm.hist + NT_;     // candidate seeds in order
@@ -1264,23 +1294,52 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
     __syncthreads();
     const bool first = tid < B && __ldcg(R.rb + sid) == tid;  // set by atomics (in L2): read past L1
     __syncthreads();
-    unsigned cand = 0;
+    unsigned cand = 0, single = 0;
     if (first) {
       R.rb[sid] = 0xFFFFFFFFu;
       float v;
       cand = (!mark_test(R, x, y, z) && level_member(R, S.ring, x, y, z, &v)) ? 1u : 0u;
+      // a start none of whose sides is an unmarked member is a layer of one cell: no flood fill
+      // (marks only grow and membership holds through the batch, so this stays true)
+      if (cand) {
+        single = 1u;
+        for (int d = 0; d < 4 && single; ++d) {
+          int dx, dz;
+          side4(d, dx, dz);
+          const int nx = x + dx, nz = z + dz;
+          if (R.ring_w == 0 && (nx < 0 || nz < 0)) continue;
+          if (!mark_test(R, nx, y, nz) && level_member(R, S.ring, nx, y, nz, &v)) single = 0u;
+        }
+      }
     }
     unsigned nc;
     const unsigned off = cta_scan_count(sm, cand, &nc);
-    if (cand) b_cand[off] = tid;
+    if (cand) b_cand[off] = tid | (single << 31);
     if (tid == 0) {
       s_stop = B;
       s_brk = 0;
+      s_cur = 0;  // the next candidate to level
     }
     __syncthreads();
-    // ---- the candidates in order
-    for (unsigned c = 0; c < nc; ++c) {
-      const unsigned j = b_cand[c];
+    // ---- the candidates in order; one-cell layers only count (fluid.rs:446, len < 2)
+    while (true) {
+      if (tid == 0) {
+        unsigned c = s_cur;
+        while (c < nc && (b_cand[c] >> 31)) {
+          sW.llc += 1u;
+          sW.level_cells_total += 1u;
+          if (sW.llc >= LEVEL_BUDGET) {
+            s_stop = (b_cand[c] & 0x7FFFFFFFu) + 1u;
+            s_brk = 1u;
+          }
+          ++c;
+          if (s_brk) break;
+        }
+        s_cur = c;
+      }
+      __syncthreads();
+      if (s_brk || s_cur >= nc) break;
+      const unsigned j = b_cand[s_cur];
       if (tid < 32u) {
         WS W = sW;
         W.pdelta = 0;
@@ -1304,14 +1363,18 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
         const unsigned len = level_bfs_cta(R, sm, S, s_qi, s_ql);
         level_finish_cta(R, sm, sW, S, len, cap);
       }
-      if (tid == 0 && (sW.llc >= LEVEL_BUDGET || sW.ndrain != 0u)) {
-        s_stop = j + 1u;
-        s_brk = 1u;
+      if (tid == 0) {
+        if (sW.llc >= LEVEL_BUDGET || sW.ndrain != 0u) {
+          s_stop = j + 1u;
+          s_brk = 1u;
+        }
+        s_cur += 1u;
       }
       __syncthreads();
       if (s_brk) break;
     }
-    // ---- the popped seeds
+    // ---- the popped seeds: out of the seed set, starts marked (and the sides a one-cell layer's
+    // flood fill tested)
     const unsigned stop = s_stop;
     if (tid < stop) {
       const unsigned k = R.seeds[ns - 1u - tid];
@@ -1319,6 +1382,15 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
       int sx, sy, sz;
       dom_xyz(R, b_start[tid], sx, sy, sz);
       mark_tas(R, sx, sy, sz);
+      if (single) {
+        for (int d = 0; d < 4; ++d) {
+          int dx, dz;
+          side4(d, dx, dz);
+          const int nx = sx + dx, nz = sz + dz;
+          if (R.ring_w == 0 && (nx < 0 || nz < 0)) continue;
+          if (in_dom(R, nx, sy, nz)) mark_tas(R, nx, sy, nz);
+        }
+      }
     }
     __syncthreads();
     if (tid == 0) {

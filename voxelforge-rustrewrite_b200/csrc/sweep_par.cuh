@@ -74,6 +74,7 @@ struct ParProf {
 // Per-segment constants, the same on every warp.
 struct ParTick {
   unsigned seg_start, seg_end, epoch;
+  unsigned pull_end;  // cells from here on make no attempt: the tick's budget is spent before them
   int gate;  // same-layer radius waited for before a pressure search
   int cone;  // lower-layer radius a cell waits for before it starts
   bool flip;
@@ -895,7 +896,8 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
   const float v0 = vol;
   if (live) {
     bool attempt = false;
-    if (vol < FULL) attempt = mode == PM_PULL || (mode == PM_SEQ && seq_pulls < MAX_PULLS_PER_TICK);
+    // in a segment with pulls, cells from T.pull_end on come after the budget's last attempt
+    if (vol < FULL) attempt = (mode == PM_PULL && i < T.pull_end) || (mode == PM_SEQ && seq_pulls < MAX_PULLS_PER_TICK);
     if (attempt) {
       co.flags |= RF_ATTEMPT;
       if (mode == PM_SEQ) seq_pulls += 1;
