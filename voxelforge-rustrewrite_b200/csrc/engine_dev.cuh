@@ -998,6 +998,23 @@ __device__ __forceinline__ bool mark_tas(const Region& R, int x, int y, int z) {
   return (old >> (bit & 31)) & 1u;
 }
 
+// LayerMarks::test_and_set of a cell known to be unmarked, in two halves so that the caller's other
+// loads overlap them: mark_begin sets the bit (no result wanted) and reads the tile's listed flag,
+// mark_end lists the tile if nobody has.
+__device__ __forceinline__ unsigned mark_begin(const Region& R, int x, int y, int z, unsigned& tile) {
+  const unsigned xr = (unsigned)(x - R.px0), zr = (unsigned)(z - R.pz0);
+  tile = ((zr >> 6) * (unsigned)R.PY + (unsigned)y) * (unsigned)R.TX + (xr >> 6);
+  const unsigned bit = ((zr & 63u) << 6) | (xr & 63u);
+  atomicOr(&R.marks[(size_t)tile * 128u + (bit >> 5)], 1u << (bit & 31));
+  return __ldcg(R.mark_tflag + tile);  // set by atomics (in L2): read past L1
+}
+__device__ __forceinline__ void mark_end(const Region& R, unsigned tile, unsigned listed) {
+  if (listed == 0u && atomicExch(&R.mark_tflag[tile], 1u) == 0u) {
+    const unsigned k = atomicAdd(&R.ctl->mark_ntiles, 1u);
+    R.mark_list[k] = tile;
+  }
+}
+
 __device__ __forceinline__ void side4(int d, int& dx, int& dz) {  // SIDES (fluid.rs:228)
   dx = (d == 0) - (d == 1);
   dz = (d == 2) - (d == 3);

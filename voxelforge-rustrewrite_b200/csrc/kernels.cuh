@@ -1100,8 +1100,10 @@ __device__ __noinline__ unsigned level_bfs_cta(const Region& R, TickSmem& sm, Sm
           nid = dom_id(R, nx, y, nz);
           if (__ldcg(R.rb + nid) == t) {  // set by atomics (in L2): read past L1
             R.rb[nid] = 0xFFFFFFFFu;
-            mark_tas(R, nx, y, nz);
+            unsigned tile;
+            const unsigned listed = mark_begin(R, nx, y, nz, tile);  // unmarked: it won the claim
             f = level_member(R, S.ring, nx, y, nz, &v) ? 1u : 0u;
+            mark_end(R, tile, listed);
           }
         }
       }
@@ -1321,16 +1323,20 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
       s_cur = 0;  // the next candidate to level
     }
     __syncthreads();
-    // ---- the candidates in order; one-cell layers only count (fluid.rs:446, len < 2)
+    // ---- the candidates in order. One-cell layers only count (fluid.rs:446, len < 2); a start
+    // that an earlier layer's flood fill marked is skipped, as its test_and_set would return
+    // (entry bits: 31 one cell, 30 marked since the batch began, 0-29 the seed)
     while (true) {
       if (tid == 0) {
         unsigned c = s_cur;
-        while (c < nc && (b_cand[c] >> 31)) {
-          sW.llc += 1u;
-          sW.level_cells_total += 1u;
-          if (sW.llc >= LEVEL_BUDGET) {
-            s_stop = (b_cand[c] & 0x7FFFFFFFu) + 1u;
-            s_brk = 1u;
+        while (c < nc && (b_cand[c] >> 30)) {
+          if (b_cand[c] >> 31) {
+            sW.llc += 1u;
+            sW.level_cells_total += 1u;
+            if (sW.llc >= LEVEL_BUDGET) {
+              s_stop = (b_cand[c] & 0x3FFFFFFFu) + 1u;
+              s_brk = 1u;
+            }
           }
           ++c;
           if (s_brk) break;
@@ -1339,7 +1345,8 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
       }
       __syncthreads();
       if (s_brk || s_cur >= nc) break;
-      const unsigned j = b_cand[s_cur];
+      const unsigned cur = s_cur;
+      const unsigned j = b_cand[cur];
       if (tid < 32u) {
         WS W = sW;
         W.pdelta = 0;
@@ -1362,6 +1369,14 @@ __device__ __noinline__ void level_round_cta(const Region& R, TickSmem& sm, WS& 
       if (s_pend) {
         const unsigned len = level_bfs_cta(R, sm, S, s_qi, s_ql);
         level_finish_cta(R, sm, sW, S, len, cap);
+      }
+      // the later candidates this layer's flood fill marked
+      for (unsigned c = cur + 1u + tid; c < nc; c += NT_) {
+        const unsigned e = b_cand[c];
+        if (e >> 30) continue;
+        int cx, cy, cz;
+        dom_xyz(R, b_start[e], cx, cy, cz);
+        if (mark_test(R, cx, cy, cz)) b_cand[c] = e | (1u << 30);
       }
       if (tid == 0) {
         if (sW.llc >= LEVEL_BUDGET || sW.ndrain != 0u) {
