@@ -149,8 +149,26 @@ int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* out);
 /* FluidSim::partials().for_each (src/fluid.rs:165-175): every partial cell as (x,y,z) + volume,
  * in ascending (page, local index) order. Writes at most cap, *n = total. */
 int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap, uint64_t* n);
-/* FluidSim::shift (src/fluid.rs:696-720): floating origin moved by (dx, dz) voxels. */
+/* FluidSim::shift (src/fluid.rs:696-720): floating origin moved by (dx, dz) voxels. Ring worlds
+ * only, by whole ring periods (ring_w * 128 voxels: the only moves src/app/window.rs:393-408 makes,
+ * ORIGIN_STEP = 65536); pair it with SparseVolume::ring_rebase / vf_world_ring_rebase on the host.
+ * VF_ERR_RANGE otherwise. */
 int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz);
+/* Ring streaming on a live handle, on the handle's device copy of the world
+ * (SparseVolume::ring_evict / ring_paste, src/voxel/sparse_volume.rs:478-537; the host calls the
+ * same on its SparseVolume). Evict empties the ring slot holding chunk (cx, cz) (a slot not loaded:
+ * nothing) and frees its bricks' atlas slots; the partial volumes its cells held are kept per cell,
+ * as FluidSim's PartialField keeps them, and count in vf_fluid_get_stats / export / digests. A
+ * drained cell of an unloaded chunk erases its kept entry (fluid.rs:586-589). Paste evicts the
+ * slot's chunk, then writes the chunk given as a SparseVolume of 128 x (chunk_bricks_y * 8) x 128
+ * voxels (grid in the reference's encoding, 16 x chunk_bricks_y x 16 words; bricks 512 bytes each)
+ * into the slot as chunk (cx, cz); kept entries of its cells come back into its bricks. The FIFO,
+ * the level seeds and the marks are untouched, as in the reference. The chunk must lie inside the
+ * handle's cell domain (the box of the chunks loaded at upload, moved by shifts): VF_ERR_RANGE
+ * otherwise; VF_ERR_OOM when the atlas is full. */
+int vf_fluid_ring_evict(vf_fluid* h, int32_t cx, int32_t cz);
+int vf_fluid_ring_paste(vf_fluid* h, const uint32_t* chunk_grid, const uint8_t* chunk_bricks, uint64_t chunk_nbricks, int32_t chunk_bricks_y,
+                        int32_t cx, int32_t cz);
 /* FluidSim::reset (src/fluid.rs:318-320): the fluid state only; the world mirror stays, and so
  * do the cumulative counters of vf_fluid_get_stats and vf_fluid_profile. */
 int vf_fluid_reset(vf_fluid* h);

@@ -57,6 +57,8 @@ def lib():
         "orc_set_partial": (None, [P, I32, I32, I32, C.c_float]),
         "orc_shift": (None, [P, I32, I32]),
         "orc_ring_rebase": (None, [P, I32, I32]),
+        "orc_ring_evict": (None, [P, I32, I32]),
+        "orc_ring_paste": (None, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint8), C.c_uint64, I32, I32, I32]),
         "orc_reset": (None, [P]),
         "orc_idle": (C.c_int, [P]),
         "orc_active_count": (C.c_uint64, [P]),
@@ -171,6 +173,17 @@ class Oracle:
     def ring_rebase(self, dcx, dcz):
         """SparseVolume::ring_rebase: the floating origin moves by (dcx, dcz) chunks."""
         lib().orc_ring_rebase(self.h, dcx, dcz)
+
+    def ring_evict(self, cx, cz):
+        """SparseVolume::ring_evict (the FluidSim keeps its partial entries)."""
+        lib().orc_ring_evict(self.h, cx, cz)
+
+    def ring_paste(self, grid, bricks, bricks_y, cx, cz):
+        """SparseVolume::ring_paste of a 128 x (bricks_y * 8) x 128 chunk (grid words, bricks)."""
+        grid = np.ascontiguousarray(grid, np.uint32)
+        bricks = np.ascontiguousarray(bricks, np.uint8)
+        lib().orc_ring_paste(self.h, grid.ctypes.data_as(C.POINTER(C.c_uint32)), bricks.ctypes.data_as(C.POINTER(C.c_uint8)),
+                             bricks.size // 512, bricks_y, cx, cz)
 
     def reset(self):
         lib().orc_reset(self.h)

@@ -87,6 +87,15 @@ float orc_volume(orc_handle* h, int32_t x, int32_t y, int32_t z) { return h->s.v
 void orc_set_partial(orc_handle* h, int32_t x, int32_t y, int32_t z, float val) { h->s.set_partial(x, y, z, val); }
 void orc_shift(orc_handle* h, int32_t dx, int32_t dz) { h->s.shift(dx, dz); }
 void orc_ring_rebase(orc_handle* h, int32_t dcx, int32_t dcz) { h->v.ring_rebase(dcx, dcz); }
+void orc_ring_evict(orc_handle* h, int32_t cx, int32_t cz) { h->v.ring_evict(cx, cz); }
+// ring_paste of a 128 x (bricks_y * 8) x 128 chunk given as grid words and bricks
+void orc_ring_paste(orc_handle* h, const uint32_t* grid, const uint8_t* bricks, uint64_t nbricks, int32_t bricks_y, int32_t cx, int32_t cz) {
+  SparseVolume c(128, bricks_y * 8, 128);
+  c.grid.assign(grid, grid + c.grid.size());
+  c.bricks.resize(nbricks);
+  for (uint64_t i = 0; i < nbricks; ++i) std::memcpy(c.bricks[i].data(), bricks + i * 512, 512);
+  h->v.ring_paste(c, cx, cz);
+}
 void orc_reset(orc_handle* h) { h->s.reset(); }
 int orc_idle(orc_handle* h) { return h->s.idle() ? 1 : 0; }
 uint64_t orc_active_count(orc_handle* h) { return h->s.active_count(); }

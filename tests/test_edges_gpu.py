@@ -163,6 +163,54 @@ def test_shift_by_ring_periods_matches_oracle(vf, orc):
     assert o.stats()["pull_success"] > 0
 
 
+def test_ring_evict_and_paste_on_a_live_handle(vf, orc):
+    """Ring streaming without a new handle (SparseVolume::ring_evict / ring_paste,
+    sparse_volume.rs:478-537). A chunk holding half of a collapsing water block is evicted mid-flow:
+    its cells read as solid, the partial volumes it held are kept per cell as PartialField keeps
+    them, and drained cells of the unloaded chunk erase theirs (fluid.rs:586-589). It is pasted
+    back (the kept volumes return into its bricks), and later a different chunk replaces the other
+    slot's chunk in one paste. State, FIFO, seeds and partial counts match the oracle every tick."""
+    chunk = vf.World(128, 64, 128)
+    chunk.fill_box(0, 0, 0, 127, 7, 127, STONE)
+    hill = vf.World(128, 64, 128)
+    hill.fill_box(0, 0, 0, 127, 7, 127, STONE)
+    hill.fill_box(100, 8, 30, 127, 20, 70, STONE)
+    ring = vf.World.ring(4, 64)
+    for cx in (-1, 0):
+        ring.ring_paste(chunk, cx, 0)
+    ring.fill_box(-20, 8, 40, 19, 30, 59, WATER)
+    ring.fill_box(-3, 8, 45, 2, 12, 54, 0)
+    sim = vf.FluidSim(ring)
+    o = oracle_for(orc, ring)
+    for s in (sim, o):
+        s.wake(-24, 7, 36, 23, 34, 63)
+
+    def paste(c, cx, cz):
+        g, b, _ = c.arrays()
+        sim.ring_paste(c, cx, cz)
+        o.ring_paste(g, b, c.info.bricks_y, cx, cz)
+
+    kept = 0
+    for t in range(1, 91):
+        if t == 25:
+            sim.ring_evict(0, 0)
+            o.ring_evict(0, 0)
+            kept = sim.partial_count()
+        if t == 50:
+            paste(chunk, 0, 0)
+        if t == 70:
+            paste(hill, -1, 0)  # the slot's chunk (-1, 0) is evicted and replaced
+        sim.tick()
+        o.tick()
+        assert_same_digest(sim, o, t)
+        assert sim.partial_count() == o.partial_count(), t
+    assert kept > 0
+    with pytest.raises(vf.VfError) as e:
+        sim.ring_paste(chunk, 1, 0)  # beyond the handle's cell domain
+    assert e.value.code == -5
+    sim.close()
+
+
 def test_shift_rejects_other_offsets(vf):
     ring = vf.World.ring(4, 64)
     chunk = vf.World(128, 64, 128)

@@ -145,6 +145,8 @@ def lib():
         "vf_fluid_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
         "vf_fluid_export_partials": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_float), U64, C.POINTER(C.c_uint64)]),
         "vf_fluid_shift": (C.c_int, [P, I32, I32]),
+        "vf_fluid_ring_evict": (C.c_int, [P, I32, I32]),
+        "vf_fluid_ring_paste": (C.c_int, [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint8), U64, I32, I32, I32]),
         "vf_fluid_reset": (C.c_int, [P]),
         "vf_fluid_snapshot_queue": (
             C.c_int,
@@ -494,6 +496,18 @@ class FluidSim:
 
     def shift(self, dx, dz):
         self._check(lib().vf_fluid_shift(self.h, dx, dz), "shift")
+
+    def ring_evict(self, cx: int, cz: int):
+        """SparseVolume::ring_evict on the device copy of the world; the chunk's partial volumes are
+        kept per cell (the host world is evicted by the caller, as the app does)."""
+        self._check(lib().vf_fluid_ring_evict(self.h, cx, cz), "ring_evict")
+
+    def ring_paste(self, chunk: "World", cx: int, cz: int):
+        """SparseVolume::ring_paste of a 128 x ny x 128 chunk world into the device copy of the world."""
+        i = chunk.info
+        grid, bricks, _ = chunk.arrays()
+        self._check(lib().vf_fluid_ring_paste(self.h, grid.ctypes.data_as(C.POINTER(C.c_uint32)), bricks.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                              int(i.nbricks), i.bricks_y, cx, cz), "ring_paste")
 
     def reset(self):
         self._check(lib().vf_fluid_reset(self.h), "reset")

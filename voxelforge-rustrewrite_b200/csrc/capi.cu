@@ -15,6 +15,14 @@
 
 using namespace vfe;
 
+// A partial entry of a cell in an evicted ring chunk: the reference's PartialField keys entries by
+// cell, not by brick, so they outlive the chunk's bricks (and return with a paste).
+struct DetachedPartial {
+  int32_t x, y, z;
+  float v;
+  uint32_t id;  // domain cell id
+};
+
 struct vf_fluid {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -41,6 +49,9 @@ struct vf_fluid {
   float* whist = nullptr;
   unsigned* staged = nullptr;
   unsigned hpos = 0;
+  // ring streaming on a live handle: entries kept for evicted chunks, atlas slots they freed
+  std::vector<DetachedPartial> det;
+  std::vector<unsigned> free_slots;
 };
 
 // A set of regions stepped together: one CTA per region in one launch (pattern (2)).
@@ -141,6 +152,108 @@ int sync_ctl(vf_fluid* h) {
 
 // Offsets into the scratch buffer are kept 16-byte aligned (8-byte device atomics live there).
 size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+// live[k] = 1 when the k-th entry kept for an evicted ring chunk still exists (a drained cell of an
+// unloaded chunk erases it).
+int detached_live(vf_fluid* h, std::vector<uint8_t>& live) {
+  const size_t nd = h->det.size();
+  live.assign(nd, 0);
+  if (!nd) return VF_OK;
+  int rc;
+  if ((rc = ensure_scratch(h, nd * 8 + 64))) return rc;
+  unsigned* dids = (unsigned*)h->scratch;
+  unsigned* dout = dids + align16(nd * 4) / 4;
+  std::vector<unsigned> ids(nd), out(nd);
+  for (size_t k = 0; k < nd; ++k) ids[k] = h->det[k].id;
+  CK(cudaMemcpyAsync(dids, ids.data(), nd * 4, cudaMemcpyHostToDevice, h->stream));
+  k_cell_bits<<<(unsigned)std::min<size_t>((nd + 255) / 256, 1024), 256, 0, h->stream>>>(h->R.detbits, dids, (unsigned)nd, 2, dout);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out.data(), dout, nd * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t k = 0; k < nd; ++k) live[k] = out[k] ? 1 : 0;
+  return VF_OK;
+}
+
+// Set (op 1) or clear (op 0) the detbits of `ids`.
+int detached_bits(vf_fluid* h, const std::vector<unsigned>& ids, int op) {
+  if (ids.empty()) return VF_OK;
+  int rc;
+  if ((rc = ensure_scratch(h, ids.size() * 4 + 64))) return rc;
+  CK(cudaMemcpyAsync(h->scratch, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  k_cell_bits<<<(unsigned)std::min<size_t>((ids.size() + 255) / 256, 1024), 256, 0, h->stream>>>(h->R.detbits, (unsigned*)h->scratch,
+                                                                                                 (unsigned)ids.size(), op, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return VF_OK;
+}
+
+// The device's count of kept entries after a change of `delta` (the ticks' erasures included).
+int detached_count(vf_fluid* h, long long delta) {
+  if ((h->hctl->ndetached + delta) > 0xFFFFFFFFll) return fail(h, VF_ERR_OOM, "too many kept partial entries");
+  const unsigned v = (unsigned)((long long)h->hctl->ndetached + delta);
+  h->hctl->ndetached = v;
+  CK(cudaMemcpy(&h->R.ctl->ndetached, &v, 4, cudaMemcpyHostToDevice));
+  return VF_OK;
+}
+
+// SparseVolume::ring_evict (sparse_volume.rs:513-537) of ring slot `si` on the device: the slot's
+// bricks become empty and their atlas slots free; the partial volumes they held are kept per cell,
+// as the reference's PartialField keeps them. `ring` is the device ring table, updated here.
+int ring_evict_slot(vf_fluid* h, int si, std::vector<int32_t>& ring) {
+  const Region& R = h->R;
+  if (!ring[3 * si + 2]) return VF_OK;
+  const int w = R.ring_w, ocx = ring[3 * si], ocz = ring[3 * si + 1];
+  const int bx0 = (si % w) * 16, bz0 = (si / w) * 16;
+  const uint64_t nb = (uint64_t)R.bx * R.by * R.bz;
+  std::vector<uint32_t> grid(nb);
+  CK(cudaMemcpy(grid.data(), R.grid, nb * 4, cudaMemcpyDeviceToHost));
+  std::vector<unsigned> slots;
+  std::vector<uint64_t> gis;
+  for (int bz = 0; bz < 16; ++bz)
+    for (int by = 0; by < R.by; ++by)
+      for (int bx = 0; bx < 16; ++bx) {
+        const uint64_t gi = ((uint64_t)(bz0 + bz) * R.by + by) * R.bx + (bx0 + bx);
+        if (grid[gi] >= 256u) {
+          slots.push_back(grid[gi] - 256u);
+          gis.push_back(gi);
+        }
+        grid[gi] = 0u;
+      }
+  int rc;
+  if (!slots.empty()) {
+    const size_t n = slots.size();
+    if ((rc = ensure_scratch(h, align16(n * 4) + n * 2048 + 64))) return rc;
+    unsigned* dslots = (unsigned*)h->scratch;
+    float* dvol = (float*)((char*)h->scratch + align16(n * 4));
+    std::vector<float> vols(n * 512);
+    CK(cudaMemcpyAsync(dslots, slots.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+    k_gather_vol<<<(unsigned)std::min<size_t>((n * 512 + 255) / 256, 8192), 256, 0, h->stream>>>(R.avol, dslots, (unsigned)n, dvol);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(vols.data(), dvol, n * 2048, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<unsigned> ids;
+    for (size_t k = 0; k < n; ++k) {
+      const uint64_t gi = gis[k];
+      const int bx = (int)(gi % R.bx), by = (int)((gi / R.bx) % R.by), bz = (int)(gi / ((uint64_t)R.bx * R.by));
+      for (int l = 0; l < 512; ++l) {
+        const float v = vols[k * 512 + l];
+        if (!(v > 0.0f)) continue;
+        const int x = ocx * 128 + (bx % 16) * 8 + (l & 7), y = by * 8 + ((l >> 3) & 7), z = ocz * 128 + (bz % 16) * 8 + (l >> 6);
+        if (!in_dom(R, x, y, z)) continue;
+        const unsigned id = dom_id(R, x, y, z);
+        h->det.push_back({x, y, z, v, id});
+        ids.push_back(id);
+      }
+      h->free_slots.push_back(slots[k]);
+    }
+    if ((rc = detached_bits(h, ids, 1))) return rc;
+    if ((rc = detached_count(h, (long long)ids.size()))) return rc;
+  }
+  CK(cudaMemcpy(R.grid, grid.data(), nb * 4, cudaMemcpyHostToDevice));
+  ring[3 * si + 2] = 0;
+  CK(cudaMemcpy(R.ring, ring.data(), ring.size() * 4, cudaMemcpyHostToDevice));
+  return VF_OK;
+}
 
 uint64_t next_pow2(uint64_t v) {
   uint64_t p = 1;
@@ -332,6 +445,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.pextra, (MAX_CELLS_PER_TICK + 31) / 32))) return rc;
   if ((rc = dalloc(h, &R.pxlist, MAX_CELLS_PER_TICK))) return rc;
   if ((rc = dalloc(h, &R.rb, ncells, false))) return rc;
+  if (ring_w && (rc = dalloc(h, &R.detbits, words))) return rc;
   if ((rc = dalloc(h, &R.deps, (uint64_t)MAX_CELLS_PER_TICK * 16, false))) return rc;
   CK(cudaMemsetAsync(R.rb, 0xFF, ncells * 4, h->stream));
   // the parallel sweep packs search-queue coordinates in 16 bits per axis
@@ -663,10 +777,26 @@ int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap
   unsigned long long cnt = 0;
   CK(cudaMemcpyAsync(&cnt, dcount, 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  if (n) *n = cnt;
   uint64_t take = std::min<uint64_t>(cnt, cap);
   if (take && xyz) CK(cudaMemcpy(xyz, dxyz, take * 12, cudaMemcpyDeviceToHost));
   if (take && vol) CK(cudaMemcpy(vol, dvol, take * 4, cudaMemcpyDeviceToHost));
+  // entries kept for evicted ring chunks
+  std::vector<uint8_t> live;
+  if ((rc = detached_live(h, live))) return rc;
+  for (size_t k = 0; k < h->det.size(); ++k) {
+    if (!live[k]) continue;
+    if (take < cap) {
+      if (xyz) {
+        xyz[3 * take] = h->det[k].x;
+        xyz[3 * take + 1] = h->det[k].y;
+        xyz[3 * take + 2] = h->det[k].z;
+      }
+      if (vol) vol[take] = h->det[k].v;
+      ++take;
+    }
+    ++cnt;
+  }
+  if (n) *n = cnt;
   // canonical order: by (x, y, z) ascending? keep (slot, voxel) order but make it deterministic
   if (take && xyz && vol) {
     std::vector<uint64_t> idx(take);
@@ -706,6 +836,10 @@ int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz) {  // fluid.rs:696-720
     ring[i + 1] -= dz / 128;
   }
   CK(cudaMemcpy(R.ring, ring.data(), ring.size() * 4, cudaMemcpyHostToDevice));
+  for (DetachedPartial& e : h->det) {  // PartialField re-keyed (fluid.rs:697-701); ids are domain-relative
+    e.x -= dx;
+    e.z -= dz;
+  }
   // the levelling round starts over (fluid.rs:715-719)
   const unsigned nt = h->hctl->mark_ntiles;
   if (nt) {
@@ -718,6 +852,117 @@ int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz) {  // fluid.rs:696-720
   CK(cudaMemcpyAsync(&R.ctl->level_round, &zero, 4, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->dR, &h->R, sizeof(Region), cudaMemcpyHostToDevice, h->stream));
   return sync_ctl(h);
+}
+
+int vf_fluid_ring_evict(vf_fluid* h, int32_t cx, int32_t cz) {  // sparse_volume.rs:513-537
+  int rc = check(h);
+  if (rc) return rc;
+  if (!h->R.ring_w) return fail(h, VF_ERR_INVALID, "not a ring world");
+  DeviceScope scope(h->device);
+  if (scope.err != cudaSuccess) return VF_ERR_CUDA;
+  if ((rc = sync_ctl(h))) return rc;
+  const int w = h->R.ring_w;
+  std::vector<int32_t> ring(3 * w * w);
+  CK(cudaMemcpy(ring.data(), h->R.ring, ring.size() * 4, cudaMemcpyDeviceToHost));
+  return ring_evict_slot(h, (cz & (w - 1)) * w + (cx & (w - 1)), ring);
+}
+
+int vf_fluid_ring_paste(vf_fluid* h, const uint32_t* chunk_grid, const uint8_t* chunk_bricks, uint64_t chunk_nbricks, int32_t chunk_bricks_y,
+                        int32_t cx, int32_t cz) {  // sparse_volume.rs:478-510
+  int rc = check(h);
+  if (rc) return rc;
+  Region& R = h->R;
+  if (!R.ring_w || !chunk_grid || chunk_bricks_y <= 0) return fail(h, VF_ERR_INVALID, "ring paste: not a ring world or no chunk");
+  if ((int64_t)cx * 128 < R.px0 || (int64_t)cx * 128 + 128 > (int64_t)R.px0 + R.PX || (int64_t)cz * 128 < R.pz0 ||
+      (int64_t)cz * 128 + 128 > (int64_t)R.pz0 + R.PZ)
+    return fail(h, VF_ERR_RANGE, "ring paste: the chunk lies outside the handle's cell domain (the chunks loaded at upload, after shifts)");
+  DeviceScope scope(h->device);
+  if (scope.err != cudaSuccess) return VF_ERR_CUDA;
+  if ((rc = sync_ctl(h))) return rc;
+  const int w = R.ring_w, si = (cz & (w - 1)) * w + (cx & (w - 1));
+  std::vector<int32_t> ring(3 * w * w);
+  CK(cudaMemcpy(ring.data(), R.ring, ring.size() * 4, cudaMemcpyDeviceToHost));
+  if ((rc = ring_evict_slot(h, si, ring))) return rc;  // whatever the slot held
+  // kept entries of this chunk's cells that no tick erased come back with it
+  std::vector<uint8_t> live;
+  if ((rc = detached_live(h, live))) return rc;
+  std::vector<DetachedPartial> keep;
+  std::vector<std::vector<std::pair<int, float>>> brick_parts(16 * 16 * (size_t)R.by);
+  std::vector<unsigned> back;
+  for (size_t k = 0; k < h->det.size(); ++k) {
+    if (!live[k]) continue;  // erased while its chunk was away
+    const DetachedPartial& e = h->det[k];
+    if ((e.x >> 7) != cx || (e.z >> 7) != cz || e.y / 8 >= std::min(R.by, chunk_bricks_y)) {
+      keep.push_back(e);
+      continue;
+    }
+    const int bx = (e.x & 127) >> 3, by = e.y >> 3, bz = (e.z & 127) >> 3;
+    brick_parts[((size_t)bz * R.by + by) * 16 + bx].push_back({(e.z & 7) * 64 + (e.y & 7) * 8 + (e.x & 7), e.v});
+    back.push_back(e.id);
+  }
+  const uint64_t nb = (uint64_t)R.bx * R.by * R.bz;
+  std::vector<uint32_t> grid(nb);
+  CK(cudaMemcpy(grid.data(), R.grid, nb * 4, cudaMemcpyDeviceToHost));
+  const int bx0 = (si % w) * 16, bz0 = (si / w) * 16;
+  std::vector<unsigned> slots;
+  std::vector<uint8_t> mats;
+  std::vector<float> vols;
+  unsigned used = h->hctl->atlas_used;
+  for (int bz = 0; bz < 16; ++bz)
+    for (int by = 0; by < std::min(R.by, chunk_bricks_y); ++by)
+      for (int bx = 0; bx < 16; ++bx) {
+        const uint32_t g = chunk_grid[((size_t)bz * chunk_bricks_y + by) * 16 + bx];
+        if (g >= 256u && (g - 256u >= chunk_nbricks || !chunk_bricks)) return fail(h, VF_ERR_INVALID, "ring paste: grid names a brick out of range");
+        const auto& parts = brick_parts[((size_t)bz * R.by + by) * 16 + bx];
+        const uint64_t gi = ((uint64_t)(bz0 + bz) * R.by + by) * R.bx + (bx0 + bx);
+        if (g < 256u && parts.empty()) {
+          grid[gi] = g;
+          continue;
+        }
+        unsigned slot;
+        if (!h->free_slots.empty()) {
+          slot = h->free_slots.back();
+          h->free_slots.pop_back();
+        } else {
+          if (used >= R.atlas_cap) return fail(h, VF_ERR_OOM, "ring paste: brick atlas full");
+          slot = used++;
+        }
+        slots.push_back(slot);
+        const size_t o = mats.size();
+        mats.resize(o + 512);
+        vols.resize(o + 512, 0.0f);
+        if (g < 256u) std::memset(&mats[o], (int)g, 512);
+        else std::memcpy(&mats[o], chunk_bricks + (size_t)(g - 256u) * 512, 512);
+        for (const auto& pr : parts) vols[o + pr.first] = pr.second;
+        grid[gi] = 256u + slot;
+      }
+  if (!slots.empty()) {
+    const size_t n = slots.size();
+    if ((rc = ensure_scratch(h, align16(n * 4) + n * 512 + n * 2048 + 64))) return rc;
+    unsigned* dslots = (unsigned*)h->scratch;
+    uint8_t* dm = (uint8_t*)h->scratch + align16(n * 4);
+    float* dv = (float*)(dm + n * 512);
+    CK(cudaMemcpyAsync(dslots, slots.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dm, mats.data(), n * 512, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dv, vols.data(), n * 2048, cudaMemcpyHostToDevice, h->stream));
+    k_scatter_bricks<<<(unsigned)std::min<size_t>((n * 512 + 255) / 256, 8192), 256, 0, h->stream>>>(R.amat, R.avol, dslots, (unsigned)n, dm, dv);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  if (used != h->hctl->atlas_used) {
+    h->hctl->atlas_used = used;
+    CK(cudaMemcpy(&R.ctl->atlas_used, &used, 4, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(R.grid, grid.data(), nb * 4, cudaMemcpyHostToDevice));
+  ring[3 * si] = cx;
+  ring[3 * si + 1] = cz;
+  ring[3 * si + 2] = 1;
+  CK(cudaMemcpy(R.ring, ring.data(), ring.size() * 4, cudaMemcpyHostToDevice));
+  // the returned entries live in the atlas again; erased ones are gone for good
+  if ((rc = detached_bits(h, back, 0))) return rc;
+  if ((rc = detached_count(h, -(long long)back.size()))) return rc;
+  h->det.swap(keep);
+  return VF_OK;
 }
 
 int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
@@ -737,6 +982,8 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   CK(cudaMemsetAsync(R.stamp, 0xFF, (size_t)R.ncells * 4, h->stream));
   CK(cudaMemsetAsync(R.zrow, 0xFF, (size_t)R.PY * R.PZ * 4, h->stream));
   CK(cudaMemsetAsync(R.ptbits, 0, words * 4, h->stream));
+  if (R.detbits) CK(cudaMemsetAsync(R.detbits, 0, words * 4, h->stream));  // kept entries go with the rest
+  h->det.clear();
   Ctl c = *h->hctl;
   Ctl z{};
   z.atlas_used = c.atlas_used;
@@ -807,7 +1054,7 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
   int rc = check(h);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
-  if ((rc = ensure_scratch(h, 64))) return rc;
+  if ((rc = ensure_scratch(h, 64 + h->det.size() * 20 + 32))) return rc;
   unsigned long long* d = (unsigned long long*)h->scratch;
   CK(cudaMemsetAsync(d, 0, 24, h->stream));
   const Region& R = h->R;
@@ -817,6 +1064,23 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
   if (ql) k_list_digest<<<(unsigned)std::min<uint64_t>((ql + 255) / 256, 4096), 256, 0, h->stream>>>(R, R.queue, ql, h->hctl->qhead, R.qmask, d + 1);
   uint64_t sl = h->hctl->nseeds;
   if (sl) k_list_digest<<<(unsigned)((sl + 255) / 256), 256, 0, h->stream>>>(R, R.seeds, sl, 0, 0xFFFFFFFFFFFFFFFFull, d + 2);
+  if (!h->det.empty()) {  // entries kept for evicted ring chunks, hashed as cells outside the loaded chunks
+    const size_t nd = h->det.size();
+    std::vector<int4> ent(nd);
+    std::vector<unsigned> ids(nd);
+    for (size_t k = 0; k < nd; ++k) {
+      unsigned vb;
+      std::memcpy(&vb, &h->det[k].v, 4);
+      ent[k] = make_int4(h->det[k].x, h->det[k].y, h->det[k].z, (int)vb);
+      ids[k] = h->det[k].id;
+    }
+    int4* dent = (int4*)((char*)h->scratch + 64);
+    unsigned* dids = (unsigned*)((char*)h->scratch + 64 + nd * 16);
+    CK(cudaMemcpyAsync(dent, ent.data(), nd * 16, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dids, ids.data(), nd * 4, cudaMemcpyHostToDevice, h->stream));
+    k_detached_digest<<<(unsigned)std::min<size_t>((nd + 255) / 256, 1024), 256, 0, h->stream>>>(R, dent, dids, (unsigned)nd, d);
+    CK(cudaStreamSynchronize(h->stream));
+  }
   CK(cudaGetLastError());
   unsigned long long out[3];
   CK(cudaMemcpyAsync(out, d, 24, cudaMemcpyDeviceToHost, h->stream));

@@ -60,6 +60,7 @@ struct Ctl {
   unsigned int pxn;                 // parallel sweep: positions listed in Region::pxlist this tick
   unsigned int att_ratio;           // parallel sweep: pull attempts per possible attempter of the
                                     // last tick's completed segments, x 65536 (0: none yet)
+  unsigned int ndetached;           // ring worlds: partial entries kept for evicted chunks (detbits set)
   // parallel sweep diagnostics, summed over ticks: budget segments run, segments rolled back and
   // replayed in order by one warp, cells replayed
   unsigned long long par_segments, par_rollbacks, par_replayed;
@@ -166,6 +167,7 @@ struct Region {
   unsigned* pxlist;      // MAX_CELLS_PER_TICK: the positions whose pextra bit is set
   unsigned* rb;          // ncells: earliest writer during a segment's rollback (0xFFFFFFFF idle)
   unsigned* deps;        // MAX_CELLS_PER_TICK * 16: earlier conflicting cells of each cell (10 used)
+  unsigned* detbits;     // ring worlds: ncells bits, the cell's partial entry is kept for an evicted chunk
   Ctl* ctl;
 };
 

@@ -1496,6 +1496,26 @@ __device__ void run_ticks(const Region& R, TickSmem& sm, int n_ticks, Tune tune)
       sW.nact = sW.nseed = sW.nchg = 0;
     }
     __syncthreads();
+    // ---- ring worlds: a drained cell of an evicted chunk is solid (outside), and the sweep erases its
+    // partial entry (fluid.rs:586-589); entries kept for evicted chunks are erased here, which nothing
+    // in the tick can tell apart (an outside cell's volume reads 0)
+    if (R.detbits && vld(&R.ctl->ndetached) != 0u) {
+      unsigned long long er = 0;
+      for (unsigned i = tid; i < n; i += NT_) {
+        const unsigned id = R.queue[(qh + i) & R.qmask];
+        int x, y, z;
+        dom_xyz(R, id, x, y, z);
+        if (!outside(R, ring, x, y, z)) continue;
+        const unsigned bit = 1u << (id & 31u);
+        if (atomicAnd(R.detbits + (id >> 5), ~bit) & bit) ++er;
+      }
+      er = cta_sum(sm, er);
+      if (tid == 0) {
+        R.ctl->partial_count -= (long long)er;
+        R.ctl->ndetached -= (unsigned)er;
+      }
+      __syncthreads();
+    }
     lap(0);
     // ---- sort (fluid.rs:575-580)
     cta_radix_sort(R.cells, R.cells_tmp, n, sm.hist, sm.sred);
@@ -1855,6 +1875,44 @@ __global__ void k_state_digest(Region R, unsigned long long* out) {
   }
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULLMASK, acc, o);
   if ((threadIdx.x & 31u) == 0) atomicAdd(out, acc);
+}
+
+// Partial entries kept for evicted ring chunks (x, y, z, volume bits, cell id per entry) whose cell
+// still has its detbits bit: hashed like cells outside the loaded chunks (material 0).
+__global__ void k_detached_digest(Region R, const int4* ent, const unsigned* ids, unsigned n, unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned id = ids[i];
+    if (!((R.detbits[id >> 5] >> (id & 31u)) & 1u)) continue;
+    const int4 e = ent[i];
+    acc += cell_hash(e.x, e.y, e.z, 0u, (unsigned)e.w);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(FULLMASK, acc, o);
+  if ((threadIdx.x & 31u) == 0) atomicAdd(out, acc);
+}
+
+// Ring paste/evict helpers: gather the partial volumes of atlas slots; write whole bricks (materials
+// and volumes) into slots; set, clear or read bits of cells.
+__global__ void k_gather_vol(const float* avol, const unsigned* slots, unsigned n, float* out) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n * 512u; t += gridDim.x * blockDim.x)
+    out[t] = avol[(size_t)slots[t >> 9] * 512u + (t & 511u)];
+}
+__global__ void k_scatter_bricks(unsigned char* amat, float* avol, const unsigned* slots, unsigned n, const unsigned char* mats,
+                                 const float* vols) {
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n * 512u; t += gridDim.x * blockDim.x) {
+    const size_t o = (size_t)slots[t >> 9] * 512u + (t & 511u);
+    amat[o] = mats[t];
+    avol[o] = vols[t];
+  }
+}
+// op 0: clear, 1: set, 2: read into out
+__global__ void k_cell_bits(unsigned* bits, const unsigned* ids, unsigned n, int op, unsigned* out) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned id = ids[i], bit = 1u << (id & 31u);
+    if (op == 0) atomicAnd(bits + (id >> 5), ~bit);
+    else if (op == 1) atomicOr(bits + (id >> 5), bit);
+    else out[i] = (bits[id >> 5] & bit) ? 1u : 0u;
+  }
 }
 
 // Order-dependent digest of a list of domain ids: sum fmix64(ref_key * golden + position).
