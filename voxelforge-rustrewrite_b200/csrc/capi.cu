@@ -80,7 +80,10 @@ struct DeviceScope {
 
 // The tick kernel of the handle's engine for `nreg` regions: one CTA per region.
 cudaError_t launch_tick(const Tune& t, Region* regs, int nreg, int n_ticks, int smem, cudaStream_t st) {
-  if (t.engine) k_tick_par<<<(unsigned)nreg, PAR_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
+  if (t.engine) {
+    const int warps = (t.gate >> 16) & 0x1F;
+    k_tick_par<<<(unsigned)nreg, warps ? 32 * warps : PAR_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
+  }
   else k_tick<<<(unsigned)nreg, TICK_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
   return cudaGetLastError();
 }
@@ -1185,8 +1188,9 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
 }
 
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap) {
-  if (!h || engine < 0 || engine > 1 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 16) ||
-      spin_cap == 0)
+  const int warps = (gate >> 16) & 0x1F;
+  if (!h || engine < 0 || engine > 1 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 21) ||
+      (warps != 0 && (warps < 8 || warps > MAX_WARPS)) || spin_cap == 0)
     return VF_ERR_INVALID;
   if (engine == 1 && h->uploaded && (h->R.PX >= 65536 || h->R.PZ >= 65536 || h->R.PY >= 65536))
     return fail(h, VF_ERR_RANGE, "the parallel sweep needs domain sides below 65536");

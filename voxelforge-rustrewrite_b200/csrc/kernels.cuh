@@ -140,7 +140,7 @@ struct Tune {
   int producers;  // one-warp sweep: 1 .. TICK_WARPS-1 prefetching warps
   int depth;      // one-warp sweep: 1 .. PF_RING cells ahead
   int engine;     // 0 one-warp sweep (TICK_THREADS per region), 1 parallel sweep (PAR_THREADS)
-  int gate;       // parallel sweep: 0 .. GATE_MAX
+  int gate;       // parallel sweep: bits 0-7 gate radius, 8-15 cone radius (0..GATE_MAX), 16-20 warps (0: MAX_WARPS)
   unsigned long long spin_cap;  // iterations before a wait gives up (ST_TIMEOUT)
 };
 
@@ -683,7 +683,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
   }
   __syncthreads();
   const int gate = max(0, min(tune.gate & 0xFF, GATE_MAX));
-  const int cone = tune.gate >> 8 ? max(0, min((tune.gate >> 8) & 0xFF, GATE_MAX)) : gate;
+  const int cone = (tune.gate >> 8) & 0xFF ? min((tune.gate >> 8) & 0xFF, GATE_MAX) : gate;
   __shared__ unsigned s_extra;
   // attempts per possible attempter over this tick's completed pull segments (the last tick's to
   // start with), for sizing the next segment
