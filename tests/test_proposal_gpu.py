@@ -70,9 +70,11 @@ def test_proposal_on_engine_traces_beats_persistence_and_keeps_state_exact(vf):
     proposal.train(mlp, X[tr].contiguous(), Y[tr].contiguous(), torch, epochs=8, batch=4096, lr=2e-3)
     s = proposal.score(mlp.forward(X[te].contiguous(), torch), Y[te])
     base = proposal.score(B[te], Y[te])
-    # the network finds more of the bricks that wake than "it woke last tick" at useful precision
-    assert s.recall > base.recall, (s, base)
-    assert s.precision > 0.5, s
+    # the network finds more of the bricks that wake than "it woke last tick" (measured on these
+    # traces: recall 0.919 vs 0.915, precision 0.985 vs 0.981; training is deterministic), at a
+    # precision no lower than the rule's and above 0.95
+    assert s.recall >= base.recall + 0.003, (s, base)
+    assert s.precision >= max(0.95, base.precision), (s, base)
     # staging the proposal's bricks changes nothing the fluid computes
     wl = vf.Workload(1)
     a, b = vf.FluidSim(wl.world(0)), vf.FluidSim(wl.world(0))
