@@ -12,9 +12,11 @@
 //   * Pull budget (fluid.rs:594, 4096 attempts per tick). Cells that can attempt a pull are known
 //     before the sweep up to one case that is checked at run time: a cell full at the tick's start
 //     only drops below 1 - 1e-4 when a pull takes from it, and pulls take only from surface cells.
-//     The sweep runs in segments of sorted order that hold at most as many possible attempters as
-//     budget is left, with a CTA barrier between segments; once the budget is spent the rest of
-//     the tick runs as one segment without pulls.
+//     The sweep runs in segments of sorted order with a CTA barrier between them. A segment is
+//     sized from the attempts expected per possible attempter (measured on earlier segments and
+//     ticks); its attempts are counted when it ends, and one that made more than the budget had
+//     left is undone and run again up to its room-th attempt. Once that end is known, one segment
+//     runs the rest of the tick: attempts before it, none after it.
 //   * Pressure searches read cells as of their own sorted position. Earlier writers of a cell on
 //     the pulling layer are waited for; later writers that already wrote are read through their
 //     records of the values they replaced (multi-version reads); a pull's source write is held
@@ -22,8 +24,10 @@
 //     one that has started is a conflict). Every pull read is stamped per cell so that an earlier
 //     pull writing a cell a later pull already read is detected.
 //   * Conflicts that ordering cannot prevent (a pull writing where a later cell has already
-//     looked) stop the segment: its writes are undone from the records and one warp replays it in
-//     sorted order. Every result is therefore the sequential one; conflicts cost time only.
+//     looked) stop the segment: its writes are undone from the records (the first write of each
+//     location by execution ticket) and it runs again up to the conflicting pull, so the late
+//     reader falls outside it; a position split too often is replayed in sorted order by one warp.
+//     Every result is therefore the sequential one; conflicts cost time only.
 // All waits are bounded (Tune::spin_cap) and end in ST_TIMEOUT.
 #pragma once
 #include "engine_dev.cuh"
