@@ -376,6 +376,9 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
     R.PZ = (cz1 - cz0 + 1) * 128 + 2 * P;
   }
   R.PY = ny + P;
+  R.mx = udiv_magic((unsigned)R.PX);
+  R.my = udiv_magic((unsigned)R.PY);
+  R.mz = udiv_magic((unsigned)R.PZ);
   uint64_t ncells = (uint64_t)R.PX * R.PY * R.PZ;
   if (ncells >= 0x7FFFFFF0ull) return fail(h, VF_ERR_RANGE, "domain too large for 31-bit cell ids");
   R.ncells = (unsigned)ncells;

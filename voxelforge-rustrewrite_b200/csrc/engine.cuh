@@ -121,6 +121,7 @@ struct Region {
   // ---- geometry (voxel dims, brick dims, ring width; padded scheduler domain)
   int nx, ny, nz, bx, by, bz, ring_w;
   int px0, pz0, PX, PY, PZ;  // domain: x in [px0, px0+PX), y in [0, PY), z in [pz0, pz0+PZ)
+  unsigned mx, my, mz;       // ceil(2^32 / PX), ceil(2^32 / PY), ceil(2^32 / PZ): see udiv
   int TX, TZ;                // layer-mark tiles (64x64) per row / column
   unsigned int ncells;       // PX*PY*PZ
   // ---- world mirror
@@ -187,6 +188,20 @@ __host__ __device__ inline unsigned long long fmix64(unsigned long long k) {
 }
 
 // ------------------------------------------------------------------------ domain ids
+// n / d for n < 2^31 and d >= 2, with m = ceil(2^32 / d): umulhi(n, m) is n / d or one more (its
+// error is below n / 2^32 < 1/2), and one compare corrects it. Cell ids and sort keys are below 2^31.
+__host__ __device__ inline unsigned udiv(unsigned n, unsigned d, unsigned m) {
+#ifdef __CUDA_ARCH__
+  unsigned q = __umulhi(n, m);
+  if (q * d > n) --q;
+  return q;
+#else
+  (void)m;
+  return n / d;
+#endif
+}
+__host__ inline unsigned udiv_magic(unsigned d) { return (unsigned)(((1ull << 32) + d - 1ull) / d); }
+
 __host__ __device__ inline bool in_dom(const Region& R, int x, int y, int z) {
   return (unsigned)(x - R.px0) < (unsigned)R.PX && (unsigned)y < (unsigned)R.PY && (unsigned)(z - R.pz0) < (unsigned)R.PZ;
 }
@@ -194,9 +209,9 @@ __host__ __device__ inline unsigned dom_id(const Region& R, int x, int y, int z)
   return ((unsigned)(z - R.pz0) * (unsigned)R.PY + (unsigned)y) * (unsigned)R.PX + (unsigned)(x - R.px0);
 }
 __host__ __device__ inline void dom_xyz(const Region& R, unsigned id, int& x, int& y, int& z) {
-  unsigned t = id / (unsigned)R.PX;
+  unsigned t = udiv(id, (unsigned)R.PX, R.mx);
   x = (int)(id - t * (unsigned)R.PX) + R.px0;
-  unsigned zz = t / (unsigned)R.PY;
+  unsigned zz = udiv(t, (unsigned)R.PY, R.my);
   y = (int)(t - zz * (unsigned)R.PY);
   z = (int)zz + R.pz0;
 }
@@ -213,9 +228,9 @@ __host__ __device__ inline unsigned sort_key(const Region& R, unsigned id, bool 
   return ((unsigned)y * (unsigned)R.PZ + zr) * (unsigned)R.PX + xr;
 }
 __host__ __device__ inline unsigned key_to_id(const Region& R, unsigned key, bool flip) {
-  unsigned t = key / (unsigned)R.PX;
+  unsigned t = udiv(key, (unsigned)R.PX, R.mx);
   unsigned xr = key - t * (unsigned)R.PX;
-  unsigned y = t / (unsigned)R.PZ;
+  unsigned y = udiv(t, (unsigned)R.PZ, R.mz);
   unsigned zr = t - y * (unsigned)R.PZ;
   if (flip) {
     xr = (unsigned)R.PX - 1u - xr;

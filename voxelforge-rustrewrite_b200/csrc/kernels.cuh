@@ -292,7 +292,11 @@ __device__ __forceinline__ bool act_cell(const Region& R, unsigned word, int o, 
     case 1: id = c + 1u; return true;
     case 2: id = c - 1u; return true;
     case 3: id = c + px; return true;
-    case 4: id = c - px; return ((c / px) % (unsigned)R.PY) != 0u;  // y - 1 < 0
+    case 4: {  // y - 1 < 0
+      id = c - px;
+      const unsigned t = udiv(c, px, R.mx);
+      return t != udiv(t, (unsigned)R.PY, R.my) * (unsigned)R.PY;
+    }
     case 5: id = c + pxy; return true;
     default: id = c - pxy; return true;
   }
@@ -316,9 +320,19 @@ __device__ void commit_acts(const Region& R, TickSmem& sm, unsigned n, unsigned 
     unsigned newmask = 0, w = 0;
     if (i < n) {
       w = R.ev_act[i];
-      unsigned id;
+      // the word's cells, then all their stamps and active words in flight together
+      unsigned ids[7], st[7], ac[7];
+      bool ok[7];
+#pragma unroll
+      for (int o = 0; o < 7; ++o) ok[o] = act_cell(R, w, o, ids[o]);
+#pragma unroll
+      for (int o = 0; o < 7; ++o) {
+        st[o] = ok[o] ? R.stamp[ids[o]] : 0xFFFFFFFFu;
+        ac[o] = ok[o] ? R.active[ids[o] >> 5] : 0u;
+      }
+#pragma unroll
       for (int o = 0; o < 7; ++o)
-        if (act_cell(R, w, o, id) && R.stamp[id] == i * 8u + (unsigned)o && !((R.active[id >> 5] >> (id & 31)) & 1u)) newmask |= 1u << o;
+        if (ok[o] && st[o] == i * 8u + (unsigned)o && !((ac[o] >> (ids[o] & 31u)) & 1u)) newmask |= 1u << o;
     }
     unsigned total;
     unsigned off = cta_scan_count(sm, __popc(newmask), &total);
@@ -618,9 +632,13 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
       const unsigned key = R.cells[i];
       const unsigned cid = key_to_id(R, key, flip);
       R.stamp[cid] = i;
-      rowflag = (i == 0u || key / (unsigned)R.PX != R.cells[i - 1u] / (unsigned)R.PX) ? 1u : 0u;
+      rowflag = (i == 0u || udiv(key, (unsigned)R.PX, R.mx) != udiv(R.cells[i - 1u], (unsigned)R.PX, R.mx)) ? 1u : 0u;
       dom_xyz(R, cid, x, y, z);
-      const CD c = load_cell(R, ring, x, y, z);
+      // the cell and the PEXPOSE + 1 cells over it, loads issued together
+      CD col[PEXPOSE + 2];
+#pragma unroll
+      for (int d = 0; d <= PEXPOSE + 1; ++d) col[d] = load_cell(R, ring, x, y + d, z);
+      const CD c = col[0];
       S = cd_solid(c) ? 1u : 0u;
       if (!S) {
         // A cell attempts only below 1 - 1e-4. One full at the tick's start gets there only as a
@@ -629,11 +647,9 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
         // cell. Cells with at most PEXPOSE water cells over them are counted; a deeper exposure
         // in one tick is caught when the pull runs (a conflict).
         P = cd_volume(c) < FULL ? 1u : 0u;
-        for (int d = 1; d <= PEXPOSE + 1 && !P; ++d) {
-          const CD u = load_cell(R, ring, x, y + d, z);
-          if (cd_solid(u) || cd_volume(u) <= 0.0f) P = 1u;
-          else if (d == PEXPOSE + 1) break;
-        }
+#pragma unroll
+        for (int d = 1; d <= PEXPOSE + 1; ++d)
+          if (!P && (cd_solid(col[d]) || cd_volume(col[d]) <= 0.0f)) P = 1u;
       }
     }
     unsigned trow, tp;
@@ -663,9 +679,23 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
     R.ctl->ptn = 0u;
   }
   // earlier conflicting cells of every cell (the position map is complete now)
-  for (unsigned t = tid; t < n * 16u; t += NT_) {
-    const unsigned i = t >> 4, l = t & 15u;
-    R.deps[t] = l < 10u ? dep_rank(R, i, flip, l) : NOSLOT;
+  for (unsigned i = tid; i < n; i += NT_) {  // one cell per thread: ten position loads in flight
+    const unsigned cid = key_to_id(R, R.cells[i], flip);
+    int x, y, z;
+    dom_xyz(R, cid, x, y, z);
+    unsigned d[16];
+#pragma unroll
+    for (unsigned l = 0; l < 10u; ++l) {
+      int dx, dy, dz;
+      dep_offset(l, flip, dx, dy, dz);
+      const unsigned r = rank_at(R, x + dx, y + dy, z + dz);
+      d[l] = r < i ? r : NOSLOT;
+    }
+#pragma unroll
+    for (unsigned l = 10u; l < 16u; ++l) d[l] = NOSLOT;
+    uint4* o = reinterpret_cast<uint4*>(R.deps + (size_t)i * 16u);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = make_uint4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
   }
   for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
   for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
@@ -776,7 +806,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
         const unsigned a = max(rs, T.seg_start), b = min(R.rowstart[t + 1u], T.seg_end);
         // publish the row and its next cell for cone_wait (key / PX = y * PZ + sorted z)
         const unsigned ka = R.cells[a];
-        const unsigned yz = ka / (unsigned)R.PX, yy = yz / (unsigned)R.PZ, zs = yz - yy * (unsigned)R.PZ;
+        const unsigned yz = udiv(ka, (unsigned)R.PX, R.mx), yy = udiv(yz, (unsigned)R.PZ, R.mz), zs = yz - yy * (unsigned)R.PZ;
         const unsigned zr = flip ? (unsigned)R.PZ - 1u - zs : zs;
         const unsigned long long rowtag = ((unsigned long long)yy << 48) | ((unsigned long long)zr << 32);
         w_fetch += (unsigned long long)(clock64() - f0);
@@ -894,7 +924,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
     const unsigned key = R.cells[i];
     const unsigned cid = key_to_id(R, key, flip);
     R.stamp[cid] = 0xFFFFFFFFu;
-    if (i == 0u || key / (unsigned)R.PX != R.cells[i - 1u] / (unsigned)R.PX) {
+    if (i == 0u || udiv(key, (unsigned)R.PX, R.mx) != udiv(R.cells[i - 1u], (unsigned)R.PX, R.mx)) {
       int x, y, z;
       dom_xyz(R, cid, x, y, z);
       R.zrow[(size_t)y * (unsigned)R.PZ + (unsigned)(z - R.pz0)] = NOSLOT;

@@ -1040,15 +1040,12 @@ __device__ __forceinline__ bool rb_write(const Region& R, const ParSmem& ps, uns
   return true;
 }
 
-// The earlier drained cells the cell at sorted position i conflicts with (lanes 0..9 of a warp
-// hold one each; NOSLOT where there is none): earlier rows of its layer (x-1, x, x+1 one row back,
-// x two rows back, mirrored on odd ticks), the five cells of the layer below under its plus
-// footprint, and the cell two below (whose start test reads the cell this one falls into).
-__device__ __forceinline__ unsigned dep_rank(const Region& R, unsigned i, bool flip, unsigned l) {
-  const unsigned cid = key_to_id(R, R.cells[i], flip);
-  int x, y, z;
-  dom_xyz(R, cid, x, y, z);
-  int dx = 0, dy = 0, dz = 0;
+// Offset of the l-th (0..9) position whose earlier drained cell a cell conflicts with: earlier rows
+// of its layer (x-1, x, x+1 one row back, x two rows back, mirrored on odd ticks), the five cells of
+// the layer below under its plus footprint, and the cell two below (whose start test reads the cell
+// this one falls into).
+__device__ __forceinline__ void dep_offset(unsigned l, bool flip, int& dx, int& dy, int& dz) {
+  dx = dy = dz = 0;
   if (l < 4u) {
     const int s = flip ? 1 : -1;
     dz = l == 3u ? 2 * s : s;
@@ -1058,13 +1055,9 @@ __device__ __forceinline__ unsigned dep_rank(const Region& R, unsigned i, bool f
     dy = -1;
     dx = (q == 1u) - (q == 2u);
     dz = (q == 3u) - (q == 4u);
-  } else if (l == 9u) {
-    dy = -2;
   } else {
-    return NOSLOT;
+    dy = -2;  // 9
   }
-  const unsigned r = rank_at(R, x + dx, y + dy, z + dz);
-  return r < i ? r : NOSLOT;
 }
 
 // Undo the writes of segment [a, b), CTA-wide: every cell written in the segment gets back the
