@@ -254,7 +254,7 @@ def test_plain_and_batched_modes_agree(vf):
     stream = torch.cuda.Stream()
     wl = vf.Workload(5, 0.05, 9)
     a = runner.make_sims(vf, wl, stream.cuda_stream)
-    b = runner.make_sims(vf, wl, stream.cuda_stream, tune=(2, 16))
+    b = runner.make_sims(vf, wl, stream.cuda_stream, tune={"engine": 0, "producers": 2, "depth": 16})
     ra = runner.run_plain(vf, wl, a, 0, 25, torch, stream)
     rb = runner.run_batched(vf, wl, b, 0, 25, torch, stream)
     assert ra.cells == rb.cells
