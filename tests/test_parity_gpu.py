@@ -323,7 +323,8 @@ def test_deep_lake_searches_hit_their_budgets(vf, orc):
 
 
 def test_tuning_knobs_never_change_results(vf, orc):
-    """Prefetch warps and prefetch distance change speed only: two extreme settings give the
+    """The knobs change speed only: the one-warp engine with extreme prefetch settings and the
+    parallel engine with several schedule shapes (gate and cone radii, 8 or 16 warps) all give the
     oracle's state on a batch of regions."""
     import torch
 
@@ -332,13 +333,15 @@ def test_tuning_knobs_never_change_results(vf, orc):
     wl = vf.Workload(3, 0.1, 4)
     stream = torch.cuda.Stream()
     digests = []
-    for tune in ((1, 1), (7, 64), (3, 16)):
+    knobs = [{"engine": 0, "producers": 1, "depth": 1}, {"engine": 0, "producers": 7, "depth": 64}, {"engine": 0, "producers": 3, "depth": 16},
+             {"engine": 1, "gate": 2}, {"engine": 1, "gate": 4 | (1 << 8)}, {"engine": 1, "gate": 8 | (4 << 8) | (8 << 16)}]
+    for tune in knobs:
         sims = runner.make_sims(vf, wl, stream.cuda_stream, tune=tune)
         runner.run_batched(vf, wl, sims, 0, 12, torch, stream)
         digests.append([s.digest() for s in sims])
         for s in sims:
             s.close()
-    assert digests[0] == digests[1] == digests[2]
+    assert all(d == digests[0] for d in digests)
     oracles = []
     for r in range(wl.regions):
         o = oracle_for(orc, wl.world(r))
