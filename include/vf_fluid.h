@@ -215,8 +215,10 @@ int vf_mlp_train_step(vf_mlp* m, const void* dev_x_f16, const float* dev_y, uint
 int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
 
 /* Which sweep runs FluidSim::tick's cell loop (src/fluid.rs:584-651); results never depend on it.
+ * engine 2 (default): chosen per tick call from the last calls' pressure-search entries per drained
+ * cell (above 1.5: engine 0, else engine 1; a batch launch uses its first handle's last choice).
  * engine 0: one warp walks the sorted cells (8 warps per region: the sweep and prefetchers).
- * engine 1 (default): all 16 warps of the region's CTA walk rows of the sorted order at once, each
+ * engine 1: all 16 warps of the region's CTA walk rows of the sorted order at once, each
  * cell waiting for the earlier cells it conflicts with; pressure searches read cells as of their own
  * position; a segment whose order the schedule cannot keep is undone and replayed by one warp.
  * gate: bits 0-7 (0..31, default 4) before a pressure search, wait for the earlier cells of its layer

@@ -390,8 +390,8 @@ class FluidSim:
         """Launch knobs of the one-warp sweep (prefetch warps, prefetch distance); results never depend on them."""
         self._check(lib().vf_fluid_set_tuning(self.h, producers, depth), "set_tuning")
 
-    def set_sweep(self, engine: int = 1, gate: int = 4 | (1 << 8), spin_cap: int = 1 << 24):
-        """Which sweep runs (0 one warp, 1 all warps of the region's CTA), the parallel sweep's pull
+    def set_sweep(self, engine: int = 2, gate: int = 4 | (1 << 8), spin_cap: int = 1 << 24):
+        """Which sweep runs (0 one warp, 1 all warps of the region's CTA, 2 chosen per call), the parallel sweep's pull
         gate radius and the iteration cap of device waits; results never depend on them."""
         self._check(lib().vf_fluid_set_sweep(self.h, engine, gate, spin_cap), "set_sweep")
 

@@ -52,6 +52,9 @@ struct vf_fluid {
   // ring streaming on a live handle: entries kept for evicted chunks, atlas slots they freed
   std::vector<DetachedPartial> det;
   std::vector<unsigned> free_slots;
+  // engine chosen per launch from the last launches' pressure-search entries per cell-step
+  bool auto_engine = true;
+  uint64_t auto_cells = 0, auto_bfs = 0;
 };
 
 // A set of regions stepped together: one CTA per region in one launch (pattern (2)).
@@ -560,6 +563,15 @@ int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks) {
   h->hzero[0] = 0u;
   CK(cudaMemcpyAsync(&h->R.ctl->changed, h->hzero, sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
   if (n_ticks > 0) {
+    if (h->auto_engine) {
+      // pull-heavy water (deep lakes, many pressure searches per cell) runs faster on the one-warp
+      // sweep; everything else on the parallel sweep. Counters as of the last synchronisation.
+      const uint64_t dc = h->hctl->cells_total - h->auto_cells, db = h->hctl->bfs_visits - h->auto_bfs;
+      const bool wide_ok = h->R.PX < 65536 && h->R.PZ < 65536 && h->R.PY < 65536;
+      if (dc > 0) h->tune.engine = (wide_ok && 2 * db <= 3 * dc) ? 1 : 0;
+      h->auto_cells = h->hctl->cells_total;
+      h->auto_bfs = h->hctl->bfs_visits;
+    }
     CK(launch_tick(h->tune, h->dR, 1, n_ticks, h->smem_bytes, h->stream));
   }
   return VF_OK;
@@ -1192,12 +1204,13 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
 
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap) {
   const int warps = (gate >> 16) & 0x1F;
-  if (!h || engine < 0 || engine > 1 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 21) ||
+  if (!h || engine < 0 || engine > 2 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 21) ||
       (warps != 0 && (warps < 8 || warps > MAX_WARPS)) || spin_cap == 0)
     return VF_ERR_INVALID;
   if (engine == 1 && h->uploaded && (h->R.PX >= 65536 || h->R.PZ >= 65536 || h->R.PY >= 65536))
     return fail(h, VF_ERR_RANGE, "the parallel sweep needs domain sides below 65536");
-  h->tune.engine = engine;
+  h->auto_engine = engine == 2;
+  if (engine != 2) h->tune.engine = engine;
   h->tune.gate = gate;
   h->tune.spin_cap = spin_cap;
   return VF_OK;
