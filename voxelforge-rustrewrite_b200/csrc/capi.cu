@@ -485,6 +485,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
 int vf_fluid_apply_voxel_edits(vf_fluid* h, const vf_voxel* edits, uint64_t n) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (!n) return VF_OK;
   if (!edits) return VF_ERR_INVALID;
   if ((rc = ensure_scratch(h, n * 16))) return rc;
@@ -504,6 +505,7 @@ int vf_fluid_apply_voxel_edits(vf_fluid* h, const vf_voxel* edits, uint64_t n) {
 int vf_fluid_wake(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (x1 < x0 || y1 < y0 || z1 < z0) return VF_OK;  // empty box: the reference's loops do nothing
   y0 = std::max(y0, 0);                            // activate ignores y < 0 (fluid.rs:293)
   if (y1 < y0) return VF_OK;
@@ -558,6 +560,7 @@ int vf_fluid_set_partial(vf_fluid* h, int32_t x, int32_t y, int32_t z, float v) 
 int vf_fluid_tick_async(vf_fluid* h, int32_t n_ticks) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (n_ticks < 0) return VF_ERR_INVALID;
   // the step's control input (reset of the "changed" flag) goes host -> device from pinned memory
   h->hzero[0] = 0u;
@@ -588,6 +591,7 @@ int vf_fluid_tick(vf_fluid* h, int32_t n_ticks, int32_t* changed) {
 int vf_fluid_sync(vf_fluid* h) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   return sync_ctl(h);
 }
 
@@ -596,6 +600,7 @@ void* vf_fluid_stream(vf_fluid* h) { return h ? (void*)h->stream : nullptr; }
 int vf_fluid_idle(vf_fluid* h, int32_t* out) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if (out) *out = (h->hctl->qtail == h->hctl->qhead && h->hctl->nseeds == 0) ? 1 : 0;  // fluid.rs:265-267
   return VF_OK;
@@ -703,6 +708,7 @@ __global__ void k_gather_changes_tail(Region R, unsigned long long total, unsign
 int vf_fluid_download_changes_noalloc(vf_fluid* h, vf_voxel* out, uint64_t cap, uint64_t* n) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (out && cap > VF_NOALLOC_MAX_CHANGES) {
     char b[160];
     snprintf(b, sizeof b, "download_changes_noalloc: cap %llu exceeds its fixed buffer of %d changes per call",
@@ -725,6 +731,7 @@ int vf_fluid_download_changes_noalloc(vf_fluid* h, vf_voxel* out, uint64_t cap, 
 int vf_fluid_volume(vf_fluid* h, int32_t x, int32_t y, int32_t z, float* out) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (!out) return VF_ERR_INVALID;
   if ((rc = ensure_scratch(h, 64))) return rc;
   k_export_box<<<1, 32, 0, h->stream>>>(h->R, x, y, z, 1, 1, 1, (unsigned char*)h->scratch, (float*)((char*)h->scratch + 16));
@@ -742,6 +749,7 @@ int vf_fluid_volume(vf_fluid* h, int32_t x, int32_t y, int32_t z, float* out) {
 int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* o) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (!o) return VF_ERR_INVALID;
   if ((rc = sync_ctl(h))) return rc;
   const Ctl& c = *h->hctl;
@@ -776,6 +784,7 @@ int vf_fluid_get_stats(vf_fluid* h, vf_fluid_stats* o) {
 int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap, uint64_t* n) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   unsigned nslots = std::min(h->hctl->atlas_used, h->R.atlas_cap);
   const size_t o_count = align16((size_t)nslots * 4), o_xyz = o_count + 64, o_vol = o_xyz + align16(cap * 12);
@@ -837,6 +846,7 @@ int vf_fluid_export_partials(vf_fluid* h, int32_t* xyz, float* vol, uint64_t cap
 int vf_fluid_shift(vf_fluid* h, int32_t dx, int32_t dz) {  // fluid.rs:696-720
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   // Ring worlds move their origin by whole ring periods (sparse_volume.rs:194-203): the brick
   // slots then stay where they are, only coordinates change. Cell ids are relative to the padded
   // domain's origin, so moving the origin re-keys the FIFO, seeds and partials at once.
@@ -986,6 +996,7 @@ int vf_fluid_ring_paste(vf_fluid* h, const uint32_t* chunk_grid, const uint8_t* 
 int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   const Region& R = h->R;
   if ((rc = sync_ctl(h))) return rc;
   unsigned used = h->hctl->atlas_used;
@@ -1028,6 +1039,7 @@ int vf_fluid_reset(vf_fluid* h) {  // fluid.rs:318-320: the fluid's tables only
 int vf_fluid_snapshot_queue(vf_fluid* h, int32_t* q_xyz, uint64_t q_cap, uint64_t* nq, int32_t* s_xyz, uint64_t s_cap, uint64_t* ns) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   const Region& R = h->R;
   uint64_t len = h->hctl->qtail - h->hctl->qhead;
@@ -1055,6 +1067,7 @@ int vf_fluid_snapshot_queue(vf_fluid* h, int32_t* q_xyz, uint64_t q_cap, uint64_
 int vf_fluid_export_box(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t sx, int32_t sy, int32_t sz, uint8_t* mat, float* part) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (sx <= 0 || sy <= 0 || sz <= 0) return VF_ERR_INVALID;
   uint64_t n = (uint64_t)sx * sy * sz;
   if ((rc = ensure_scratch(h, n * 5 + 64))) return rc;
@@ -1071,6 +1084,7 @@ int vf_fluid_export_box(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t
 int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* seeds) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if ((rc = ensure_scratch(h, 64 + h->det.size() * 20 + 32))) return rc;
   unsigned long long* d = (unsigned long long*)h->scratch;
@@ -1112,6 +1126,7 @@ int vf_fluid_digest(vf_fluid* h, uint64_t* state, uint64_t* queue, uint64_t* see
 int vf_fluid_profile(vf_fluid* h, uint64_t* out16) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if (out16) std::memcpy(out16, h->hctl->prof, 16 * sizeof(uint64_t));
   return VF_OK;
@@ -1146,6 +1161,7 @@ static int proposal_buffers(vf_fluid* h) {
 int vf_fluid_proposal_features(vf_fluid* h, void* dev_x, uint64_t cap_slots, uint64_t* nslots) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = proposal_buffers(h))) return rc;
   if ((rc = sync_ctl(h))) return rc;
   const unsigned n = std::min(h->hctl->atlas_used, h->R.atlas_cap);
@@ -1166,6 +1182,7 @@ int vf_fluid_proposal_features(vf_fluid* h, void* dev_x, uint64_t cap_slots, uin
 int vf_fluid_proposal_labels(vf_fluid* h, uint32_t since_tick, float* dev_y, uint64_t nslots) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if (!nslots) return VF_OK;
   if (!dev_y) return VF_ERR_INVALID;
@@ -1180,6 +1197,7 @@ int vf_fluid_proposal_labels(vf_fluid* h, uint32_t since_tick, float* dev_y, uin
 int vf_fluid_stage_bricks(vf_fluid* h, const float* dev_prob, uint64_t nslots, float threshold, uint64_t* n_staged) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = proposal_buffers(h))) return rc;
   if (!nslots) return VF_OK;
   const unsigned n = (unsigned)std::min<uint64_t>(nslots, h->R.atlas_cap);
@@ -1233,6 +1251,7 @@ int vf_fluid_set_log_caps(vf_fluid* h, uint32_t act, uint32_t seed, uint32_t chg
 int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out18) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if (out18) std::memcpy(out18, h->hctl->pprof, 18 * sizeof(uint64_t));
   return VF_OK;
@@ -1241,6 +1260,7 @@ int vf_fluid_sweep_profile(vf_fluid* h, uint64_t* out18) {
 int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, uint64_t* replayed, uint64_t* conflicts3) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if ((rc = sync_ctl(h))) return rc;
   if (segments) *segments = h->hctl->par_segments;
   if (rollbacks) *rollbacks = h->hctl->par_rollbacks;
@@ -1255,6 +1275,7 @@ int vf_fluid_sweep_stats(vf_fluid* h, uint64_t* segments, uint64_t* rollbacks, u
 int vf_fluid_emit_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, float amount) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   k_edit<<<1, 32, 0, h->stream>>>(h->R, ED_EMIT, dev_xyz, n, 0, amount, nullptr);
   CK(cudaGetLastError());
   return VF_OK;
@@ -1263,6 +1284,7 @@ int vf_fluid_emit_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, 
 int vf_fluid_brush_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n, uint8_t m) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   k_edit<<<1, 32, 0, h->stream>>>(h->R, ED_BRUSH, dev_xyz, n, m, 0.0f, nullptr);
   CK(cudaGetLastError());
   return VF_OK;
@@ -1271,6 +1293,7 @@ int vf_fluid_brush_device_async(vf_fluid* h, const int32_t* dev_xyz, uint64_t n,
 int vf_fluid_wake_async(vf_fluid* h, int32_t x0, int32_t y0, int32_t z0, int32_t x1, int32_t y1, int32_t z1) {
   int rc = check(h);
   if (rc) return rc;
+  DeviceScope scope(h->device);  // the caller's current device is given back on return
   if (x1 < x0 || y1 < y0 || z1 < z0) return VF_OK;
   y0 = std::max(y0, 0);
   if (y1 < y0) return VF_OK;
@@ -1288,6 +1311,7 @@ int vf_batch_create(vf_fluid* const* hs, int32_t n, vf_batch** out) {
     if (rc) return rc;
     if (hs[i]->device != h->device) return fail(h, VF_ERR_INVALID, "batched handles must share a device");
   }
+  DeviceScope scope(h->device);
   auto* b = new vf_batch();
   b->hs.assign(hs, hs + n);
   b->stream = h->stream;
@@ -1308,6 +1332,7 @@ int vf_batch_create(vf_fluid* const* hs, int32_t n, vf_batch** out) {
 
 void vf_batch_destroy(vf_batch* b) {
   if (!b) return;
+  DeviceScope scope(b->hs[0]->device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->dregs) cudaFree(b->dregs);
@@ -1317,6 +1342,7 @@ void vf_batch_destroy(vf_batch* b) {
 int vf_batch_tick_async(vf_batch* b, int32_t n_ticks) {
   if (!b || n_ticks < 0) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   if (n_ticks) {
     CK(launch_tick(h->tune, b->dregs, (int)b->hs.size(), n_ticks, h->smem_bytes, b->stream));
   }
@@ -1326,6 +1352,7 @@ int vf_batch_tick_async(vf_batch* b, int32_t n_ticks) {
 int vf_batch_sync(vf_batch* b) {
   if (!b) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   CK(cudaStreamSynchronize(b->stream));
   for (vf_fluid* x : b->hs) {
     int rc = sync_ctl(x);
@@ -1338,6 +1365,7 @@ int vf_batch_sync(vf_batch* b) {
 int vf_batch_capture(vf_batch* b, int32_t launches, int32_t ticks_per_launch) {
   if (!b || launches <= 0 || ticks_per_launch <= 0) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   if (b->exec) {
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
@@ -1360,6 +1388,7 @@ int vf_batch_capture(vf_batch* b, int32_t launches, int32_t ticks_per_launch) {
 int vf_batch_begin_capture(vf_batch* b) {
   if (!b) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   for (vf_fluid* x : b->hs)
     if (x->stream != b->stream) return fail(h, VF_ERR_INVALID, "capture needs every handle on the batch's stream");
   if (b->exec) {
@@ -1377,6 +1406,7 @@ int vf_batch_begin_capture(vf_batch* b) {
 int vf_batch_end_capture(vf_batch* b) {
   if (!b) return VF_ERR_INVALID;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
   if (e != cudaSuccess) return fail(h, VF_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
   CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
@@ -1386,6 +1416,7 @@ int vf_batch_end_capture(vf_batch* b) {
 int vf_batch_replay(vf_batch* b) {
   if (!b || !b->exec) return VF_ERR_STATE;
   vf_fluid* h = b->hs[0];
+  DeviceScope scope(h->device);
   CK(cudaGraphLaunch(b->exec, b->stream));
   return VF_OK;
 }
@@ -1399,6 +1430,7 @@ int vf_fluid_batch_tick(vf_fluid* const* hs, int32_t n, int32_t n_ticks) {
     if (rc) return rc;
     if (hs[i]->device != h->device) return fail(h, VF_ERR_INVALID, "batched handles must share a device");
   }
+  DeviceScope scope(h->device);
   std::vector<Region> regs(n);
   for (int i = 0; i < n; ++i) regs[i] = hs[i]->R;
   int rc;
