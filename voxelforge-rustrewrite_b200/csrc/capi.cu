@@ -82,10 +82,15 @@ struct DeviceScope {
 };
 
 // The tick kernel of the handle's engine for `nreg` regions: one CTA per region.
+// The parallel sweep uses only the parallel member of TickSmem's union: its launch asks for that
+// much shared memory, which leaves the rest of the SM's 256 KB to L1.
+constexpr int PAR_SMEM_BYTES = (int)((offsetof(TickSmem, u) + sizeof(ParSmem) + 127) / 128 * 128);
+static_assert(PAR_SMEM_BYTES <= (int)sizeof(TickSmem), "parallel sweep shared memory");
+
 cudaError_t launch_tick(const Tune& t, Region* regs, int nreg, int n_ticks, int smem, cudaStream_t st) {
   if (t.engine) {
     const int warps = (t.gate >> 16) & 0x1F;
-    k_tick_par<<<(unsigned)nreg, warps ? 32 * warps : PAR_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
+    k_tick_par<<<(unsigned)nreg, warps ? 32 * warps : PAR_THREADS, PAR_SMEM_BYTES, st>>>(regs, nreg, n_ticks, t);
   }
   else k_tick<<<(unsigned)nreg, TICK_THREADS, smem, st>>>(regs, nreg, n_ticks, t);
   return cudaGetLastError();
@@ -324,7 +329,7 @@ int vf_fluid_create(const vf_fluid_desc* desc, vf_fluid** out) {
   }
   h->smem_bytes = (int)sizeof(TickSmem);
   cudaFuncSetAttribute(k_tick, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_bytes);
-  cudaFuncSetAttribute(k_tick_par, cudaFuncAttributeMaxDynamicSharedMemorySize, h->smem_bytes);
+  cudaFuncSetAttribute(k_tick_par, cudaFuncAttributeMaxDynamicSharedMemorySize, PAR_SMEM_BYTES);
   *out = h;
   return VF_OK;
 }
@@ -456,6 +461,7 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.rb, ncells, false))) return rc;
   if (ring_w && (rc = dalloc(h, &R.detbits, words))) return rc;
   if ((rc = dalloc(h, &R.deps, (uint64_t)MAX_CELLS_PER_TICK * 16, false))) return rc;
+  if ((rc = dalloc(h, &R.pcg, MAX_WARPS, false))) return rc;
   CK(cudaMemsetAsync(R.rb, 0xFF, ncells * 4, h->stream));
   // the parallel sweep packs search-queue coordinates in 16 bits per axis
   if (R.PX >= 65536 || R.PZ >= 65536 || R.PY >= 65536) h->tune.engine = 0;

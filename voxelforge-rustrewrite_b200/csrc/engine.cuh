@@ -169,6 +169,7 @@ struct Region {
   unsigned* rb;          // ncells: earliest writer during a segment's rollback (0xFFFFFFFF idle)
   unsigned* deps;        // MAX_CELLS_PER_TICK * 16: earlier conflicting cells of each cell (10 used)
   unsigned* detbits;     // ring worlds: ncells bits, the cell's partial entry is kept for an evicted chunk
+  struct PullCtx* pcg;   // one pressure-search context per sweep warp (used when the shared pool is empty)
   Ctl* ctl;
 };
 

@@ -700,7 +700,9 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
   for (unsigned w = tid; w < (n + 3u) / 4u; w += NT_) ps.state[w] = 0u;
   for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
   if (tid == 0) R.ctl->pxn = 0u;
-  for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
+  for (unsigned t = tid; t < NPC_SMEM * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
+  for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) R.pcg[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
+  if (tid == 0) ps.pc_free = (1u << NPC_SMEM) - 1u;
   __syncthreads();
   plap(0);
   // ---- budget segments
@@ -788,7 +790,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
       if (warp == 0) {
         unsigned sp = s_c;
         unsigned cgi = 0xFFFFFFFFu, cg = 0u;
-        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, ps.pc[0], ring, T, PM_SEQ, i, sp, pf, NOSLOT, cgi, cg, NOSLOT, 0u);
+        for (unsigned i = T.seg_start; i < T.seg_end; ++i) process_cell_par(R, ps, R.pcg[0], ring, T, PM_SEQ, i, sp, pf, NOSLOT, cgi, cg, NOSLOT, 0u, R.cells[i]);
         if (lane == 0) R.ctl->par_replayed += T.seg_end - T.seg_start;
       }
       __syncthreads();
@@ -813,11 +815,15 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
         bool ok = true;
         unsigned cgi = 0xFFFFFFFFu, cg = 0u;
         unsigned jr_next = R.deps[a * 16u + (lane & 15u)];
+        unsigned key_next = ka;
         for (unsigned i = a; i < b && ok; ++i) {
-          const unsigned jr = jr_next;
-          if (i + 1u < b) jr_next = R.deps[(i + 1u) * 16u + (lane & 15u)];  // used by the next cell
-          if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = rowtag | (R.cells[i] - yz * (unsigned)R.PX);
-          ok = process_cell_par(R, ps, ps.pc[warp], ring, T, mode, i, seq_pulls, pf, jr, cgi, cg, t, rs);
+          const unsigned jr = jr_next, key = key_next;
+          if (i + 1u < b) {  // used by the next cell
+            jr_next = R.deps[(i + 1u) * 16u + (lane & 15u)];
+            key_next = R.cells[i + 1u];
+          }
+          if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = rowtag | (key - yz * (unsigned)R.PX);
+          ok = process_cell_par(R, ps, R.pcg[warp], ring, T, mode, i, seq_pulls, pf, jr, cgi, cg, t, rs, key);
         }
         if (lane == 0) *(volatile unsigned long long*)&ps.wrow[warp] = WROW_IDLE;
         if (!ok || vld(&ps.abort)) break;
@@ -1643,8 +1649,13 @@ __global__ void __launch_bounds__(PAR_THREADS, 1) k_tick_par(Region* regs, int n
   extern __shared__ __align__(16) unsigned char smraw[];
   TickSmem& sm = *reinterpret_cast<TickSmem*>(smraw);
   tune.engine = 1;
+  // The region's constants (sizes, array bases) are read on every cell of the sweep: a copy in
+  // shared memory keeps them off the L1, which the sweep's records and atlas lines stream through.
+  __shared__ Region s_reg;
   for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
-    run_ticks(regs[r], sm, n_ticks, tune);
+    if (threadIdx.x == 0) s_reg = regs[r];
+    __syncthreads();
+    run_ticks(s_reg, sm, n_ticks, tune);
     __syncthreads();
   }
 }

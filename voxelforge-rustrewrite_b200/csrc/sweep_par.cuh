@@ -51,9 +51,15 @@ struct PullCtx {
   unsigned vis[PV_CAP];       // visited cell ids (EMPTY_ID = free)
 };
 
+// Pressure searches in flight at once are few (a search is ~4% of a worker warp's time on the dam
+// break), so shared memory holds a small pool of search contexts; a warp that finds the pool empty
+// runs its search on its own context in global memory (Region::pcg) and never waits. Keeping the
+// pool small leaves the SM's L1 most of its 256 KB for the footprint loads.
+constexpr int NPC_SMEM = 4;
 struct ParSmem {
   unsigned state[(MAX_CELLS_PER_TICK + 3) / 4];  // one byte per drained cell: blockers / CS_*
-  PullCtx pc[MAX_WARPS];
+  PullCtx pc[NPC_SMEM];
+  unsigned pc_free;  // bit c: shared search context c is free
   unsigned next_task, task_end, abort, viol;
   unsigned viol_pos;  // smallest sorted position of a pull that met a conflict
   unsigned ticket;    // execution order of write groups in the segment (rollback restores the first)
@@ -86,6 +92,14 @@ struct ParTick {
 };
 
 __device__ __forceinline__ unsigned vld(const unsigned* p) { return *(volatile const unsigned*)p; }
+// A global word that only this CTA's threads write (grid words, row progress, pull stamps and
+// registries): a relaxed load at CTA scope. It is coherent with the CTA's stores and atomics, as
+// volatile is, but may be served by the SM's L1 instead of a round trip to L2.
+__device__ __forceinline__ unsigned gld(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.cta.global.u32 %0, [%1];" : "=r"(v) : "l"(__cvta_generic_to_global(p)));
+  return v;
+}
 __device__ __forceinline__ void vst(unsigned* p, unsigned v) { *(volatile unsigned*)p = v; }
 
 // Back-off of a polling loop after n polls: a few polls at full rate, then sleeps growing from 32 ns
@@ -184,7 +198,7 @@ __device__ __forceinline__ CD load_cell_par(const Region& R, const int* ring, in
   c.out = outside(R, ring, x, y, z);
   if (c.out) return c;
   c.gi = grid_index(R, x >> 3, y >> 3, z >> 3);
-  unsigned g = vld(R.grid + c.gi);
+  unsigned g = gld(R.grid + c.gi);
   unsigned long long spins = 0;
   while (g == GRID_LOCKED) {
     if (++spins > cap) {
@@ -193,7 +207,7 @@ __device__ __forceinline__ CD load_cell_par(const Region& R, const int* ring, in
       return c;
     }
     backoff(spins);
-    g = vld(R.grid + c.gi);
+    g = gld(R.grid + c.gi);
   }
   __threadfence_block();
   if (g < 256u) {
@@ -225,7 +239,7 @@ __device__ __forceinline__ CD load_cell_cached(const Region& R, const int* ring,
   if (c.gi == cgi && cg >= 256u && cg != GRID_LOCKED) {
     g = cg;
   } else {
-    g = vld(R.grid + c.gi);
+    g = gld(R.grid + c.gi);
     unsigned long long spins = 0;
     while (g == GRID_LOCKED) {
       if (++spins > cap) {
@@ -234,7 +248,7 @@ __device__ __forceinline__ CD load_cell_cached(const Region& R, const int* ring,
         return c;
       }
       backoff(spins);
-      g = vld(R.grid + c.gi);
+      g = gld(R.grid + c.gi);
     }
     __threadfence_block();
     cgi = c.gi;
@@ -263,7 +277,7 @@ __device__ void materialize_par(const Region& R, bool need, unsigned gi, unsigne
   bool fill = false;
   if (leader) {
     unsigned long long spins = 0;
-    g = vld(R.grid + gi);
+    g = gld(R.grid + gi);
     while (true) {
       if (g == GRID_LOCKED) {
         if (++spins > cap) {
@@ -271,7 +285,7 @@ __device__ void materialize_par(const Region& R, bool need, unsigned gi, unsigne
           break;
         }
         backoff(spins);
-        g = vld(R.grid + gi);
+        g = gld(R.grid + gi);
         continue;
       }
       if (g >= 256u) {
@@ -365,7 +379,7 @@ __device__ void ptreg_insert(const Region& R, unsigned epoch, unsigned id, unsig
   unsigned h = (id * 2654435761u) & (PTREG_CAP - 1u);
   for (unsigned n = 0; n < 2u * PTREG_CAP; ++n) {
     PullTarget* e = R.ptreg + h;
-    const unsigned ep = vld(&e->epoch);
+    const unsigned ep = gld(&e->epoch);
     if (ep != epoch) {
       if (atomicCAS(&e->epoch, ep, epoch) == ep) {
         e->id = id;
@@ -390,9 +404,9 @@ __device__ unsigned ptreg_after(const Region& R, ParSmem& ps, const ParTick& T, 
   unsigned h = (id * 2654435761u) & (PTREG_CAP - 1u);
   for (unsigned n = 0; n < PTREG_CAP; ++n) {
     const PullTarget* e = R.ptreg + h;
-    if (vld(&e->epoch) != T.epoch) break;
+    if (gld(&e->epoch) != T.epoch) break;
     unsigned long long spins = 0;
-    while (vld(&e->ready) != T.epoch) {
+    while (gld(&e->ready) != T.epoch) {
       if (++spins > T.spin_cap) {
         par_timeout(R, ps, 33);
         return best;
@@ -433,7 +447,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
   }
   out.out = false;
   out.gi = grid_index(R, a >> 3, b >> 3, c >> 3);
-  unsigned g = vld(R.grid + out.gi);
+  unsigned g = gld(R.grid + out.gi);
   atomicMax(R.preader + id, ((T.epoch & 0xFFFFu) << 16) | (k + 1u));
   if (b == ky) {
     // earlier writers on the pulling layer must be done (those within the gate are already)
@@ -442,7 +456,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
 #pragma unroll
       for (int q = 0; q < 6; ++q)
         if (jr[q] != NOSLOT && jr[q] < k && jr[q] >= T.seg_start && !wait_done(R, ps, T, jr[q], 34)) return false;
-      g = vld(R.grid + out.gi);  // a writer waited for may have materialised the brick
+      g = gld(R.grid + out.gi);  // a writer waited for may have materialised the brick
     }
   }
   unsigned long long spins = 0;
@@ -452,7 +466,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
       return false;
     }
     backoff(spins);
-    g = vld(R.grid + out.gi);
+    g = gld(R.grid + out.gi);
   }
   __threadfence_block();  // one CTA runs the region: CTA scope orders every party
   if (g < 256u) {
@@ -464,7 +478,7 @@ __device__ bool read_mvcc(const Region& R, ParSmem& ps, const int* ring, const P
     out.part = R.avol[o];
   }
   __threadfence_block();
-  const unsigned ptw = vld(&R.ptbits[id >> 5]);
+  const unsigned ptw = gld(&R.ptbits[id >> 5]);
   unsigned best = NOSLOT;
   float bp = 0.0f;
   unsigned bm = 0;
@@ -614,7 +628,7 @@ __device__ bool pull_write(const Region& R, ParSmem& ps, const int* ring, const 
   // conflict (the write is undone with the segment: the record holds the old value)
   bool late = false;
   if (mode == PM_PULL && lane == 0) {
-    const unsigned v = vld(R.preader + sid);
+    const unsigned v = gld(R.preader + sid);
     if ((v >> 16) == (T.epoch & 0xFFFFu) && (v & 0xFFFFu) > k + 1u) {
       late = true;
       atomicAdd(&R.ctl->par_conflicts[1], 1ull);
@@ -790,7 +804,7 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
   bool pend = r != NOSLOT && needc > 0u;
   unsigned long long spins = 0;
   while (true) {
-    pend = pend && vld(R.rowprog + r) < needc;
+    pend = pend && gld(R.rowprog + r) < needc;
     if (!__any_sync(FULLMASK, pend)) return true;
     if (vld(&ps.abort)) return false;
     if (++spins > T.spin_cap) {
@@ -805,16 +819,17 @@ __device__ bool gate_wait(const Region& R, ParSmem& ps, const ParTick& T, int x,
 // One drained cell (fluid.rs:584-651) at sorted position i, warp-collective. PM_PULL / PM_NOPULL:
 // running beside other warps (waits, blocking, multi-version pull reads); PM_SEQ: one warp replaying
 // a segment in order, attempts counted in `seq_pulls`. Returns false when the segment stops.
+// pcw: the warp's search context in global memory (used when the shared pool is empty);
 // jr: this lane's entry of the cell's earlier conflicting cells (ParDeps, lanes 0..9); cgi / cg:
 // the lane's grid-word cache (load_cell_cached); row / rstart: the cell's row and its first sorted
-// position (row NOSLOT: looked up).
-__device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, const int* ring, const ParTick& T, int mode, unsigned i,
+// position (row NOSLOT: looked up); key: the cell's sort key (R.cells[i], loaded ahead by the caller).
+__device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pcw, const int* ring, const ParTick& T, int mode, unsigned i,
                                  unsigned& seq_pulls, ParProf& pf, unsigned jr, unsigned& cgi, unsigned& cg, unsigned row,
-                                 unsigned rstart) {
+                                 unsigned rstart, unsigned key) {
   const unsigned lane = lane_id();
   long long c0 = clock64();
   const float FULL = full_level();
-  const unsigned cid = key_to_id(R, R.cells[i], T.flip);
+  const unsigned cid = key_to_id(R, key, T.flip);
   int x, y, z;
   dom_xyz(R, cid, x, y, z);
   // ---- earlier conflicting cells: earlier rows of the layer, the layer below, two below
@@ -914,7 +929,24 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pc, cons
           c0 = c1;
         }
         bool ok = true;
+        // a search context: a free one of the shared pool, else the warp's own in global memory
+        int pcs = -1;
+        if (lane == 0) {
+          unsigned m = vld(&ps.pc_free);
+          while (m) {
+            const int b = __ffs(m) - 1;
+            const unsigned old = atomicAnd(&ps.pc_free, ~(1u << b));
+            if (old & (1u << b)) {
+              pcs = b;
+              break;
+            }
+            m = old & ~(1u << b);
+          }
+        }
+        pcs = __shfl_sync(FULLMASK, pcs, 0);
+        PullCtx& pc = pcs >= 0 ? ps.pc[pcs] : pcw;
         const float got = pull_par(R, ps, pc, ring, T, mode, i, x, y, z, __fsub_rn(1.0f, vol), fp, co, ok, pf);
+        if (lane == 0 && pcs >= 0) atomicOr(&ps.pc_free, 1u << pcs);
         if (!ok) {
           if (lane == 0 && !vld(&ps.abort)) {
             vst(&ps.viol, 1u);
