@@ -1639,8 +1639,11 @@ __global__ void __launch_bounds__(TICK_THREADS, 1) k_tick(Region* regs, int nreg
   extern __shared__ __align__(16) unsigned char smraw[];
   TickSmem& sm = *reinterpret_cast<TickSmem*>(smraw);
   tune.engine = 0;
+  __shared__ Region s_reg;  // the region's constants, as in k_tick_par
   for (int r = blockIdx.x; r < nreg; r += gridDim.x) {
-    run_ticks(regs[r], sm, n_ticks, tune);
+    if (threadIdx.x == 0) s_reg = regs[r];
+    __syncthreads();
+    run_ticks(s_reg, sm, n_ticks, tune);
     __syncthreads();
   }
 }
