@@ -37,7 +37,7 @@ DAM_BREAK = "dam-break 512x128x512, 4-octave noise terrain, lake y<48, 8-wide ch
 # DRAM bytes (read + write) of one k_tick_par launch of one step (10 dam-break ticks, ticks
 # 51..60, cold L2 as after the bench's flush): a one-off ncu capture, summarised in
 # profiles/k_tick_par_dambreak_step_dram.txt. Compare with roofline.alg_bytes_per_step.
-STEP_DRAM_BYTES = 2153728 + 268032
+STEP_DRAM_BYTES = 2570496 + 212480
 
 
 def parse():

@@ -225,7 +225,9 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth);
  * within this Chebyshev distance; bits 8-15 (0..31, 0 = the same value, default 1) a cell of a segment with
  * pulls starts only when rows in work on lower layers within that many rows have passed its x plus
  * that distance (fewer replays, less overlap); bits 16-20 (0 = 16, else 8..16) the warps of the
- * region's CTA (for measuring the speed-up against warps). spin_cap (> 0, default 2^24): iterations of any device
+ * region's CTA (for measuring the speed-up against warps); bit 21: pressure searches leave the four
+ * search contexts in shared memory unused and run on each warp's context in global memory (the path
+ * a search takes when the shared ones are all in use; for tests). spin_cap (> 0, default 2^24): iterations of any device
  * wait (both engines, and the levelling's brick materialisation) before the tick gives up with
  * VF_ERR_TIMEOUT; the kernel then returns and the handle can only be destroyed.
  * No reference counterpart: a device scheduling knob of this library. */

@@ -322,6 +322,33 @@ def test_deep_lake_searches_hit_their_budgets(vf, orc):
     assert st["bfs_visits"] > 64 * st["pull_nonempty"] > 0  # long searches (over 100 entries on average)
 
 
+@pytest.mark.parametrize("global_only", [False, True])
+def test_parallel_sweep_search_contexts(vf, orc, global_only):
+    """The parallel sweep runs pressure searches on four search contexts in shared memory, or on
+    the warp's own context in global memory when those are taken. Bit 21 of the sweep knob sends
+    every search to the global ones, so both kinds run the deep lake's long searches; state and
+    counters match the oracle every tick."""
+    w = vf.World(48, 72, 48)
+    w.fill_box(0, 0, 0, 47, 3, 47, 3)
+    w.fill_box(0, 4, 0, 47, 71, 1, 3)
+    w.fill_box(0, 4, 46, 47, 71, 47, 3)
+    w.fill_box(0, 4, 0, 1, 71, 47, 3)
+    w.fill_box(46, 4, 0, 47, 71, 47, 3)
+    w.fill_box(2, 4, 2, 45, 59, 45, 5)
+    w.fill_box(20, 0, 20, 27, 3, 27, 0)
+    sim = vf.FluidSim(w)
+    sim.set_sweep(1, 4 | (1 << 8) | ((1 << 21) if global_only else 0))
+    o = oracle_for(orc, w)
+    for s_ in (sim, o):
+        s_.wake(0, 0, 0, 47, 71, 47)
+    for t in range(25):
+        sim.tick()
+        o.tick()
+        assert_same_digest(sim, o, t + 1)
+    assert o.stats()["pull_nonempty"] > 500 and o.stats()["bfs_visits"] > 100000  # many long searches ran
+    sim.close()
+
+
 def test_tuning_knobs_never_change_results(vf, orc):
     """The knobs change speed only: the one-warp engine with extreme prefetch settings and the
     parallel engine with several schedule shapes (gate and cone radii, 8 or 16 warps) all give the

@@ -461,7 +461,11 @@ int vf_fluid_upload_world(vf_fluid* h, int32_t nx, int32_t ny, int32_t nz, int32
   if ((rc = dalloc(h, &R.rb, ncells, false))) return rc;
   if (ring_w && (rc = dalloc(h, &R.detbits, words))) return rc;
   if ((rc = dalloc(h, &R.deps, (uint64_t)MAX_CELLS_PER_TICK * 16, false))) return rc;
+  // the warps' search contexts in global memory: visited sets empty (every search empties its own
+  // before it returns)
   if ((rc = dalloc(h, &R.pcg, MAX_WARPS, false))) return rc;
+  static_assert(EMPTY_ID == 0xFFFFFFFFu, "a visited-set slot of 0xFF bytes is free");
+  CK(cudaMemsetAsync(R.pcg, 0xFF, MAX_WARPS * sizeof(PullCtx), h->stream));
   CK(cudaMemsetAsync(R.rb, 0xFF, ncells * 4, h->stream));
   // the parallel sweep packs search-queue coordinates in 16 bits per axis
   if (R.PX >= 65536 || R.PZ >= 65536 || R.PY >= 65536) h->tune.engine = 0;
@@ -1228,7 +1232,7 @@ int vf_fluid_set_tuning(vf_fluid* h, int32_t producers, int32_t depth) {
 
 int vf_fluid_set_sweep(vf_fluid* h, int32_t engine, int32_t gate, uint64_t spin_cap) {
   const int warps = (gate >> 16) & 0x1F;
-  if (!h || engine < 0 || engine > 2 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 21) ||
+  if (!h || engine < 0 || engine > 2 || gate < 0 || (gate & 0xFF) > GATE_MAX || ((gate >> 8) & 0xFF) > GATE_MAX || (gate >> 22) ||
       (warps != 0 && (warps < 8 || warps > MAX_WARPS)) || spin_cap == 0)
     return VF_ERR_INVALID;
   if (engine == 1 && h->uploaded && (h->R.PX >= 65536 || h->R.PZ >= 65536 || h->R.PY >= 65536))

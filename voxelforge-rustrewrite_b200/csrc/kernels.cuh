@@ -140,7 +140,7 @@ struct Tune {
   int producers;  // one-warp sweep: 1 .. TICK_WARPS-1 prefetching warps
   int depth;      // one-warp sweep: 1 .. PF_RING cells ahead
   int engine;     // 0 one-warp sweep (TICK_THREADS per region), 1 parallel sweep (PAR_THREADS)
-  int gate;       // parallel sweep: bits 0-7 gate radius, 8-15 cone radius (0..GATE_MAX), 16-20 warps (0: MAX_WARPS)
+  int gate;       // parallel sweep: bits 0-7 gate radius, 8-15 cone radius (0..GATE_MAX), 16-20 warps (0: MAX_WARPS), 21 global search contexts only
   unsigned long long spin_cap;  // iterations before a wait gives up (ST_TIMEOUT)
 };
 
@@ -701,8 +701,7 @@ __device__ __noinline__ void sweep_parallel(const Region& R, TickSmem& sm, WS& s
   for (unsigned w = tid; w < (n + 31u) / 32u; w += NT_) R.pextra[w] = 0u;
   if (tid == 0) R.ctl->pxn = 0u;
   for (unsigned t = tid; t < NPC_SMEM * PV_CAP; t += NT_) ps.pc[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
-  for (unsigned t = tid; t < MAX_WARPS * PV_CAP; t += NT_) R.pcg[t / PV_CAP].vis[t % PV_CAP] = EMPTY_ID;
-  if (tid == 0) ps.pc_free = (1u << NPC_SMEM) - 1u;
+  if (tid == 0) ps.pc_free = ((tune.gate >> 21) & 1) ? 0u : (1u << NPC_SMEM) - 1u;  // bit 21: global contexts only
   __syncthreads();
   plap(0);
   // ---- budget segments
