@@ -894,9 +894,11 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pcw, con
     rc->omat[lane] = mine.mat;
   }
   if (lane == 0) rc->flags = 0;
+  // every lane gets the footprint's values (volume, material, outside); the atlas slot and grid
+  // index stay with the lane that loaded the cell (`mine`), the only one that writes it
   CD fp[7];
 #pragma unroll
-  for (int l = 0; l < 7; ++l) fp[l] = shfl_cd(mine, l);
+  for (int l = 0; l < 7; ++l) fp[l] = shfl_cd_values(mine, l);
   {
     const long long c1 = clock64();
     pf.load += (unsigned long long)(c1 - c0);
@@ -933,7 +935,7 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pcw, con
         int pcs = -1;
         if (lane == 0) {
           unsigned m = vld(&ps.pc_free);
-          while (m) {
+          for (int tries = 0; m && tries < 2 * NPC_SMEM; ++tries) {
             const int b = __ffs(m) - 1;
             const unsigned old = atomicAnd(&ps.pc_free, ~(1u << b));
             if (old & (1u << b)) {
