@@ -80,19 +80,6 @@ __device__ __forceinline__ CD shfl_cd(const CD& c, int src) {
   return r;
 }
 
-// shfl_cd without the atlas slot and grid index (NOSLOT / 0 in the result): for footprints whose
-// other lanes only read the cell's volume, material and `outside`.
-__device__ __forceinline__ CD shfl_cd_values(const CD& c, int src) {
-  CD r;
-  r.part = __shfl_sync(FULLMASK, c.part, src);
-  r.slot = NOSLOT;
-  r.gi = 0;
-  const unsigned p = __shfl_sync(FULLMASK, (unsigned)c.mat | ((unsigned)c.out << 8), src);
-  r.mat = (unsigned char)(p & 255u);
-  r.out = (p >> 8) != 0;
-  return r;
-}
-
 // Warp-uniform state of one region's sweep.
 struct WS {
   unsigned long long qhead, qtail;

@@ -894,11 +894,20 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pcw, con
     rc->omat[lane] = mine.mat;
   }
   if (lane == 0) rc->flags = 0;
-  // every lane gets the footprint's values (volume, material, outside); the atlas slot and grid
-  // index stay with the lane that loaded the cell (`mine`), the only one that writes it
+  // every lane gets what the rules read of the footprint, cd_solid and cd_volume: one ballot of
+  // the solid cells and the 7 volumes (a solid cell's volume is never read). The atlas slot, grid
+  // index, material and partial entry stay with the lane that loaded the cell (`mine`).
   CD fp[7];
+  {
+    const unsigned solid = __ballot_sync(FULLMASK, cd_solid(mine));
+    const float lv = cd_volume(mine);
 #pragma unroll
-  for (int l = 0; l < 7; ++l) fp[l] = shfl_cd_values(mine, l);
+    for (int l = 0; l < 7; ++l) {
+      const float v = __shfl_sync(FULLMASK, lv, l);
+      const bool so = (solid >> l) & 1u;
+      fp[l] = CD{so ? 0.0f : v, NOSLOT, 0u, (unsigned char)0, so};  // cd_solid = so, cd_volume = v
+    }
+  }
   {
     const long long c1 = clock64();
     pf.load += (unsigned long long)(c1 - c0);
