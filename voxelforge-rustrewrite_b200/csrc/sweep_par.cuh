@@ -955,9 +955,15 @@ __device__ bool process_cell_par(const Region& R, ParSmem& ps, PullCtx& pcw, con
           }
         }
         pcs = __shfl_sync(FULLMASK, pcs, 0);
+        // a shared context passes between warps: the last user's emptied visited set is released
+        // before its free bit (fence, then atomicOr) and acquired after it (atomicAnd, then fence)
+        if (pcs >= 0) __threadfence_block();
         PullCtx& pc = pcs >= 0 ? ps.pc[pcs] : pcw;
         const float got = pull_par(R, ps, pc, ring, T, mode, i, x, y, z, __fsub_rn(1.0f, vol), fp, co, ok, pf);
-        if (lane == 0 && pcs >= 0) atomicOr(&ps.pc_free, 1u << pcs);
+        if (pcs >= 0) {
+          __threadfence_block();
+          if (lane == 0) atomicOr(&ps.pc_free, 1u << pcs);
+        }
         if (!ok) {
           if (lane == 0 && !vld(&ps.abort)) {
             vst(&ps.viol, 1u);
